@@ -1,0 +1,213 @@
+/*
+ * pdfp_b200.h -- C ABI of libpdfp_b200.so, the B200 projector and root-LP
+ * solver of the PDFP feasibility pump.
+ *
+ * The library owns every device buffer of a handle for the handle's lifetime
+ * (the whole pump run); host pointers passed in are borrowed for the duration
+ * of the call and copied.  Every entry point returns 0 on success or a
+ * negative PDFP_E* code; pdfp_last_error() gives the message of the last
+ * failure on the calling thread.  Nothing aborts the process.
+ *
+ * Each entry point cites the reference interface (MIT-Lu-Lab/PDFP v0.1.0,
+ * paths relative to its source tree) that it replaces.
+ *
+ * Indices are 0-based int32 CSR with ascending column indices per row; the
+ * reference's Julia shim converts its 1-based Int64 CSC (a transpose-free
+ * conversion: CSC of A' is the CSR of A).
+ *
+ * Threading: a handle is not re-entrant; separate handles may be used from
+ * separate threads.  All work of a handle runs on one CUDA stream owned by it.
+ */
+#ifndef PDFP_B200_H
+#define PDFP_B200_H
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PDFP_API __attribute__((visibility("default")))
+#else
+#define PDFP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+#define PDFP_OK 0
+#define PDFP_E_INVALID (-1)      /* bad argument (shape, CSR structure, NaN input) */
+#define PDFP_E_CUDA (-2)         /* CUDA runtime error */
+#define PDFP_E_NOMEM (-3)        /* device allocation failed */
+#define PDFP_E_TIMEOUT (-4)      /* a bounded device wait gave up */
+#define PDFP_E_UNSUPPORTED (-5)  /* size beyond the library's limits */
+#define PDFP_E_NODEVICE (-6)     /* no CUDA device */
+
+/* Termination reasons, the reference's Symbols (src/pdfp.jl:276-286,
+ * src/pdlp.jl:352-370). */
+#define PDFP_UNSPECIFIED 0
+#define PDFP_OPTIMAL 1
+#define PDFP_ITERATION_LIMIT 2
+#define PDFP_TIME_LIMIT 3
+#define PDFP_PRIMAL_INFEASIBLE 4
+#define PDFP_DUAL_INFEASIBLE 5
+
+/* Arithmetic of the iterations.  FP64: plain FP64 form.  MIXED: iterates,
+ * matrix values and row accumulation in FP32; KKT/gap/restart reductions,
+ * Halpern weights and the reported distance in FP64 on the device; an FP64
+ * polish takes over when the FP32 residual stalls above tolerance. */
+#define PDFP_FP64 0
+#define PDFP_MIXED 1
+
+/* Which state vector pdfp_get_vector reads (all in scaled units). */
+#define PDFP_VEC_PDHG_X 0
+#define PDFP_VEC_PDHG_Y 1
+#define PDFP_VEC_PDHG_Z 2
+#define PDFP_VEC_CURRENT_X 3
+#define PDFP_VEC_CURRENT_Y 4
+#define PDFP_VEC_CURRENT_Z 5
+#define PDFP_VEC_DUAL_SLACK 6
+#define PDFP_VEC_REFLECTED_X 7
+
+typedef struct pdfp_handle pdfp_handle;
+
+/* A sparse matrix: m rows, n columns, row_ptr[m+1], col_idx/val[row_ptr[m]]. */
+typedef struct {
+    int32_t m, n;
+    const int32_t* row_ptr;
+    const int32_t* col_idx;
+    const double* val;
+} pdfp_csr;
+
+/* SolverParameters + RestartParameters, src/pdlp.jl:10-31 (same meaning and
+ * defaults; see pdfp_default_params). */
+typedef struct {
+    double eps_optimal_relative;
+    double eps_feasible_relative;
+    int64_t iteration_limit;
+    double time_limit;
+    int32_t termination_evaluation_frequency;
+    int32_t sv_max_iterations;
+    double reflection_coefficient;
+    double sv_tolerance;
+    double artificial_restart_threshold;
+    double sufficient_reduction_for_restart;
+    double necessary_reduction_for_restart;
+    double k_p, k_i, k_d, i_smooth;
+} pdfp_params;
+
+/* Outcome of one solve (per instance for batches). */
+typedef struct {
+    int32_t status;              /* PDFP_OPTIMAL, ... (termination_reason) */
+    int32_t restarts;
+    int64_t total_count;         /* PDHG iterations of this solve (multiple of the evaluation frequency) */
+    double rel_primal, rel_dual, rel_gap;
+    double primal_weight, step_size, max_singular_value, fixed_point_error;
+    double objective_value;      /* PDLP: c'x in original units; PDFP: l1 distance sum_I w|x - x~| (scaled data) */
+    int32_t polished;            /* MIXED: iterations finished in the FP64 polish */
+    int32_t precision;           /* arithmetic at termination */
+} pdfp_result;
+
+/* One projection problem (the data of PDFPState, src/pdfp.jl:15-52), already
+ * scaled.  is_eq[m], is_int[n] are 0/1 bytes; w[n] the y-box half widths
+ * (used on is_int columns); row_unscale[m] (nullable) = 1 ./ D_r switches the
+ * primal residual to original units (original_primal_residual!). */
+typedef struct {
+    pdfp_csr A;
+    const double* b;
+    const uint8_t* is_eq;
+    const uint8_t* is_int;
+    const double* var_lb;
+    const double* var_ub;
+    const double* w;
+    const double* row_unscale;
+} pdfp_problem;
+
+/* ---- library ---------------------------------------------------------------- */
+
+/* Fill the reference defaults (src/pdlp.jl:10-31). */
+PDFP_API void pdfp_default_params(pdfp_params* p);
+/* Message of the last failure on the calling thread ("" if none). */
+PDFP_API const char* pdfp_last_error(void);
+/* Name of the CUDA device the library uses (the pump log's "device" line,
+ * src/pump.jl:442). */
+PDFP_API int pdfp_device_name(char* buf, int32_t len);
+/* Version string of this library. */
+PDFP_API const char* pdfp_version(void);
+
+/* ---- projector: PDFPState and its methods (src/pdfp.jl) ---------------------- */
+
+/* PDFPState(A, b, is_eq, is_int, var_lb, var_ub, w; use_gpu = true),
+ * src/pdfp.jl:60-76, plus original_primal_residual!(s, D_r), src/pdfp.jl:85-90
+ * when row_unscale (= 1 ./ D_r) is not NULL. */
+PDFP_API int pdfp_create(const pdfp_csr* A, const double* b, const uint8_t* is_eq, const uint8_t* is_int,
+                const double* var_lb, const double* var_ub, const double* w,
+                const double* row_unscale, int32_t precision, pdfp_handle** out);
+
+/* k independent projections packed block-diagonally into one handle: one
+ * launch sequence advances all of them, each with its own restart and
+ * termination state on the device.  Replaces the reference's concurrent
+ * trajectory processes (scripts/solve.jl:121-148) with batch members. */
+PDFP_API int pdfp_create_batch(int32_t k, const pdfp_problem* problems, int32_t precision,
+                      pdfp_handle** out);
+
+/* copyto!(s.current_x, x); copyto!(s.initial_x, x), src/pump.jl:305-306. */
+PDFP_API int pdfp_set_x(pdfp_handle* h, int32_t instance, const double* x);
+/* set_target!(s, x_tilde_scaled), src/pdfp.jl:98-101 (then warm_start!). */
+PDFP_API int pdfp_set_target(pdfp_handle* h, int32_t instance, const double* x_tilde);
+/* warm_start!(s), src/pdfp.jl:104-114. */
+PDFP_API int pdfp_warm_start(pdfp_handle* h, int32_t instance);
+/* pdfp_solve!(s, p, primal_weight), src/pdfp.jl:252-288: instance 0 of the
+ * handle (single-problem handles). */
+PDFP_API int pdfp_solve(pdfp_handle* h, const pdfp_params* p, double primal_weight, pdfp_result* r);
+/* pdfp_solve! for every member of a batch handle at once; params,
+ * primal_weights and results hold one entry per instance. */
+PDFP_API int pdfp_solve_batch(pdfp_handle* h, const pdfp_params* params, const double* primal_weights,
+                     pdfp_result* results);
+/* Read a state vector of an instance (s.pdhg_x etc., scaled units, the
+ * caller's variable/row order). */
+PDFP_API int pdfp_get_vector(pdfp_handle* h, int32_t instance, int32_t which, double* out);
+/* s.pdhg_x of an instance: the projection in scaled units (src/pump.jl:338). */
+PDFP_API int pdfp_get_x(pdfp_handle* h, int32_t instance, double* x_scaled);
+/* Instance count, rows and columns of an instance. */
+PDFP_API int pdfp_shape(const pdfp_handle* h, int32_t instance, int32_t* k, int32_t* m, int32_t* n);
+/* Release every device buffer of the handle (the Julia finalizer). */
+PDFP_API int pdfp_destroy(pdfp_handle* h);
+
+/* Kernel timing of the two fused PDHG step kernels, over `iterations` steps
+ * of instance state as it stands (benchmark support; state advances). ms_*
+ * receive the mean device time per launch. */
+PDFP_API int pdfp_profile_step(pdfp_handle* h, int32_t iterations, float* ms_primal, float* ms_dual,
+                      double* bytes_primal, double* bytes_dual);
+
+/* ---- preconditioner (src/preconditioner.jl) --------------------------------- */
+
+/* scale_problem(A, c, var_lb, var_ub, con_lb, con_ub; ruiz_iterations,
+ * pock_chambolle_alpha, bound_objective_rescaling), src/preconditioner.jl:26-99,
+ * computed on the device.  val_out has A's sparsity pattern. */
+PDFP_API int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double* var_lb,
+                       const double* var_ub, const double* con_lb, const double* con_ub,
+                       int32_t ruiz_iterations, double pock_chambolle_alpha,
+                       int32_t bound_objective_rescaling, double* val_out, double* c_out,
+                       double* var_lb_out, double* var_ub_out, double* con_lb_out,
+                       double* con_ub_out, double* D_r, double* D_c, double* bound_scale,
+                       double* objective_scale);
+
+/* estimate_max_singular_value(A, A_t, m; max_iterations, tolerance),
+ * src/preconditioner.jl:108-125, on the device. */
+PDFP_API int pdfp_estimate_max_singular_value(const pdfp_csr* A, int32_t max_iterations, double tolerance,
+                                     double* sigma, int32_t* iterations);
+
+/* ---- root LP (src/pdlp.jl) --------------------------------------------------- */
+
+/* solve_lp_relaxation(milp; tolerance, time_limit, use_gpu = true,
+ * cupdlpx_termination), src/pdlp.jl:381-393, for the canonical MILP rows
+ * (is_le[i] = 1: A_i x <= b_i, else A_i x = b_i).  x_out in original units,
+ * dual_slack_out in scaled units, as the reference returns them. */
+PDFP_API int pdlp_solve_relaxation(const pdfp_csr* A, const double* c, const double* l, const double* u,
+                          const double* b, const uint8_t* is_le, double tolerance,
+                          double time_limit, int32_t cupdlpx_termination, int32_t precision,
+                          double* x_out, double* dual_slack_out, pdfp_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,252 @@
+// api.cu -- the extern "C" entry points of libpdfp_b200.so (include/pdfp_b200.h).
+//
+// Every entry point catches the library's exceptions and returns a status
+// code; the message is kept per thread for pdfp_last_error().
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/pdfp_b200.h"
+#include "device.hpp"
+#include "projector.hpp"
+#include "solvers.hpp"
+
+namespace pdfp {
+const char* last_error_cstr();
+}
+
+struct pdfp_handle {
+    std::unique_ptr<pdfp::Projector> proj;
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        pdfp::set_last_error("");
+        f();
+        return PDFP_OK;
+    } catch (const pdfp::Error& e) {
+        pdfp::set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        pdfp::set_last_error("host allocation failed");
+        return PDFP_E_NOMEM;
+    } catch (const std::exception& e) {
+        pdfp::set_last_error(e.what());
+        return PDFP_E_INVALID;
+    }
+}
+
+void require_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) throw pdfp::Error(PDFP_E_NODEVICE, "no CUDA device available");
+}
+
+void check_csr(const pdfp_csr* A) {
+    if (!A) throw pdfp::Error(PDFP_E_INVALID, "null matrix");
+    if (A->m < 0 || A->n < 0) throw pdfp::Error(PDFP_E_INVALID, "negative dimension");
+    if (A->m > 0 && !A->row_ptr) throw pdfp::Error(PDFP_E_INVALID, "null row_ptr");
+    if (A->m > 0 && A->row_ptr[A->m] > 0 && (!A->col_idx || !A->val))
+        throw pdfp::Error(PDFP_E_INVALID, "null col_idx or val");
+}
+
+pdfp::ProblemData to_data(const pdfp_problem& p) {
+    check_csr(&p.A);
+    if ((p.A.m > 0 && (!p.b)) || (p.A.n > 0 && (!p.is_int || !p.var_lb || !p.var_ub || !p.w)))
+        throw pdfp::Error(PDFP_E_INVALID, "null problem vector");
+    static const int32_t zero_rp = 0;
+    return pdfp::ProblemData{p.A.m, p.A.n, p.A.m > 0 ? p.A.row_ptr : &zero_rp, p.A.col_idx, p.A.val,
+                             p.b, p.is_eq, p.is_int, p.var_lb, p.var_ub, p.w, p.row_unscale};
+}
+
+}  // namespace
+
+extern "C" {
+
+void pdfp_default_params(pdfp_params* p) {
+    if (!p) return;
+    p->eps_optimal_relative = 1e-4;
+    p->eps_feasible_relative = 1e-4;
+    p->iteration_limit = 100000;
+    p->time_limit = 3600.0;
+    p->termination_evaluation_frequency = 200;
+    p->sv_max_iterations = 5000;
+    p->reflection_coefficient = 1.0;
+    p->sv_tolerance = 1e-4;
+    p->artificial_restart_threshold = 0.36;
+    p->sufficient_reduction_for_restart = 0.2;
+    p->necessary_reduction_for_restart = 0.5;
+    p->k_p = 0.99;
+    p->k_i = 0.01;
+    p->k_d = 0.0;
+    p->i_smooth = 0.3;
+}
+
+const char* pdfp_last_error(void) { return pdfp::last_error_cstr(); }
+
+const char* pdfp_version(void) { return "pdfp_b200 0.1.0 (sm_100a)"; }
+
+int pdfp_device_name(char* buf, int32_t len) {
+    return guarded([&] {
+        require_device();
+        int dev = 0;
+        PDFP_CK(cudaGetDevice(&dev));
+        cudaDeviceProp prop;
+        PDFP_CK(cudaGetDeviceProperties(&prop, dev));
+        if (buf && len > 0) {
+            std::strncpy(buf, prop.name, static_cast<size_t>(len) - 1);
+            buf[len - 1] = '\0';
+        }
+    });
+}
+
+int pdfp_create(const pdfp_csr* A, const double* b, const uint8_t* is_eq, const uint8_t* is_int,
+                const double* var_lb, const double* var_ub, const double* w,
+                const double* row_unscale, int32_t precision, pdfp_handle** out) {
+    if (!A || !out) {
+        pdfp::set_last_error("null argument");
+        return PDFP_E_INVALID;
+    }
+    pdfp_problem p{*A, b, is_eq, is_int, var_lb, var_ub, w, row_unscale};
+    return pdfp_create_batch(1, &p, precision, out);
+}
+
+int pdfp_create_batch(int32_t k, const pdfp_problem* problems, int32_t precision, pdfp_handle** out) {
+    return guarded([&] {
+        if (!out || !problems || k < 1) throw pdfp::Error(PDFP_E_INVALID, "null argument or k < 1");
+        *out = nullptr;
+        if (precision != PDFP_FP64 && precision != PDFP_MIXED)
+            throw pdfp::Error(PDFP_E_INVALID, "precision must be PDFP_FP64 or PDFP_MIXED");
+        require_device();
+        std::vector<pdfp::ProblemData> data;
+        for (int32_t i = 0; i < k; ++i) data.push_back(to_data(problems[i]));
+        std::unique_ptr<pdfp_handle> h(new pdfp_handle);
+        h->proj.reset(new pdfp::Projector(data, precision));
+        *out = h.release();
+    });
+}
+
+int pdfp_set_x(pdfp_handle* h, int32_t instance, const double* x) {
+    return guarded([&] {
+        if (!h || !x) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->set_x(instance, x);
+    });
+}
+
+int pdfp_set_target(pdfp_handle* h, int32_t instance, const double* x_tilde) {
+    return guarded([&] {
+        if (!h || !x_tilde) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->set_target(instance, x_tilde);
+    });
+}
+
+int pdfp_warm_start(pdfp_handle* h, int32_t instance) {
+    return guarded([&] {
+        if (!h) throw pdfp::Error(PDFP_E_INVALID, "null handle");
+        h->proj->warm_start(instance);
+    });
+}
+
+int pdfp_solve(pdfp_handle* h, const pdfp_params* p, double primal_weight, pdfp_result* r) {
+    return guarded([&] {
+        if (!h || !p || !r) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        const int K = h->proj->instances();
+        std::vector<pdfp_params> ps(K, *p);
+        std::vector<double> pw(K, primal_weight);
+        std::vector<pdfp_result> rs(K);
+        h->proj->solve(ps.data(), pw.data(), rs.data());
+        *r = rs[0];
+    });
+}
+
+int pdfp_solve_batch(pdfp_handle* h, const pdfp_params* params, const double* primal_weights,
+                     pdfp_result* results) {
+    return guarded([&] {
+        if (!h || !params || !primal_weights || !results) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->solve(params, primal_weights, results);
+    });
+}
+
+int pdfp_get_vector(pdfp_handle* h, int32_t instance, int32_t which, double* out) {
+    return guarded([&] {
+        if (!h || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->get_vector(instance, which, out);
+    });
+}
+
+int pdfp_get_x(pdfp_handle* h, int32_t instance, double* x_scaled) {
+    return pdfp_get_vector(h, instance, PDFP_VEC_PDHG_X, x_scaled);
+}
+
+int pdfp_shape(const pdfp_handle* h, int32_t instance, int32_t* k, int32_t* m, int32_t* n) {
+    return guarded([&] {
+        if (!h) throw pdfp::Error(PDFP_E_INVALID, "null handle");
+        const int K = h->proj->instances();
+        if (k) *k = K;
+        if (instance < 0 || instance >= K) throw pdfp::Error(PDFP_E_INVALID, "instance index out of range");
+        if (m) *m = h->proj->rows(instance);
+        if (n) *n = h->proj->cols(instance);
+    });
+}
+
+int pdfp_destroy(pdfp_handle* h) {
+    return guarded([&] { delete h; });
+}
+
+int pdfp_profile_step(pdfp_handle* h, int32_t iterations, float* ms_primal, float* ms_dual,
+                      double* bytes_primal, double* bytes_dual) {
+    return guarded([&] {
+        if (!h || !ms_primal || !ms_dual || !bytes_primal || !bytes_dual)
+            throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->profile_step(iterations, ms_primal, ms_dual, bytes_primal, bytes_dual);
+    });
+}
+
+int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double* var_lb,
+                       const double* var_ub, const double* con_lb, const double* con_ub,
+                       int32_t ruiz_iterations, double pock_chambolle_alpha,
+                       int32_t bound_objective_rescaling, double* val_out, double* c_out,
+                       double* var_lb_out, double* var_ub_out, double* con_lb_out,
+                       double* con_ub_out, double* D_r, double* D_c, double* bound_scale,
+                       double* objective_scale) {
+    return guarded([&] {
+        check_csr(A);
+        require_device();
+        pdfp::scale_problem_device(*A, c, var_lb, var_ub, con_lb, con_ub, ruiz_iterations,
+                                   pock_chambolle_alpha, bound_objective_rescaling != 0, val_out,
+                                   c_out, var_lb_out, var_ub_out, con_lb_out, con_ub_out, D_r, D_c,
+                                   bound_scale, objective_scale);
+    });
+}
+
+int pdfp_estimate_max_singular_value(const pdfp_csr* A, int32_t max_iterations, double tolerance,
+                                     double* sigma, int32_t* iterations) {
+    return guarded([&] {
+        check_csr(A);
+        if (!sigma) throw pdfp::Error(PDFP_E_INVALID, "null output");
+        require_device();
+        int32_t it = 0;
+        *sigma = pdfp::estimate_sv_device(*A, max_iterations, tolerance, &it);
+        if (iterations) *iterations = it;
+    });
+}
+
+int pdlp_solve_relaxation(const pdfp_csr* A, const double* c, const double* l, const double* u,
+                          const double* b, const uint8_t* is_le, double tolerance,
+                          double time_limit, int32_t cupdlpx_termination, int32_t precision,
+                          double* x_out, double* dual_slack_out, pdfp_result* r) {
+    return guarded([&] {
+        check_csr(A);
+        if (!x_out || !dual_slack_out || !r) throw pdfp::Error(PDFP_E_INVALID, "null output");
+        require_device();
+        pdfp::solve_lp_relaxation_device(*A, c, l, u, b, is_le, tolerance, time_limit,
+                                         cupdlpx_termination != 0, precision, x_out,
+                                         dual_slack_out, r);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// device.cu -- uploads of the packed matrix and its tilings.
+#include "device.hpp"
+
+namespace pdfp {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+__global__ void f64_to_f32_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = static_cast<float>(a[i]);
+}
+
+void DeviceMatrix::upload(DeviceArena& ar, bool want_f32) {
+    rp_a = ar.upload(L.A.rp);
+    ci_a = ar.upload(L.A.ci);
+    v64_a = ar.upload(L.A.v);
+    rp_t = ar.upload(L.At.rp);
+    ci_t = ar.upload(L.At.ci);
+    v64_t = ar.upload(L.At.v);
+    row_off = ar.upload(L.row_off);
+    col_off = ar.upload(L.col_off);
+    n_eq = ar.upload(L.n_eq);
+    row_orig = ar.upload(L.row_orig);
+    col_orig = ar.upload(L.col_orig);
+    max_m = max_n = 0;
+    for (int p = 0; p < L.K; ++p) {
+        max_m = std::max(max_m, L.row_off[p + 1] - L.row_off[p]);
+        max_n = std::max(max_n, L.col_off[p + 1] - L.col_off[p]);
+    }
+    if (want_f32) {
+        v32_a = ar.alloc<float>(L.NNZ);
+        v32_t = ar.alloc<float>(L.NNZ);
+        refresh_f32(0);
+        PDFP_CK(cudaDeviceSynchronize());
+    }
+}
+
+void DeviceMatrix::refresh_f32(cudaStream_t s) {
+    if (!v32_a || L.NNZ == 0) return;
+    int blocks = static_cast<int>(std::min<int64_t>((L.NNZ + 255) / 256, 4096));
+    f64_to_f32_kernel<<<blocks, 256, 0, s>>>(v64_a, v32_a, L.NNZ);
+    f64_to_f32_kernel<<<blocks, 256, 0, s>>>(v64_t, v32_t, L.NNZ);
+    PDFP_CK(cudaGetLastError());
+}
+
+DeviceMatrix::Tiling DeviceMatrix::make_tiling(DeviceArena& ar, bool transpose,
+                                               const StageGeom& g) const {
+    Tiling t;
+    const HostCsr& csr = transpose ? L.At : L.A;
+    build_tiling(csr, transpose ? L.col_off : L.row_off, g, t.host);
+    SideDev& s = t.dev;
+    s.rows = csr.rows;
+    s.n_tiles = static_cast<int32_t>(t.host.tile_inst.size());
+    s.n_chunks = static_cast<int32_t>(t.host.chunk_k0.size());
+    s.max_tile_rows = t.host.max_tile_rows;
+    s.stage_bytes = g.stage_bytes;
+    s.rp = transpose ? rp_t : rp_a;
+    s.ci = transpose ? ci_t : ci_a;
+    s.tile_row = ar.upload(t.host.tile_row);
+    s.tile_chunk = ar.upload(t.host.tile_chunk);
+    s.tile_inst = ar.upload(t.host.tile_inst);
+    s.chunk_k0 = ar.upload(t.host.chunk_k0);
+    s.chunk_k1 = ar.upload(t.host.chunk_k1);
+    s.chunk_tile = ar.upload(t.host.chunk_tile);
+    s.chunk_flags = ar.upload(t.host.chunk_flags);
+    t.inst_tile0 = ar.upload(t.host.inst_tile0);
+    return t;
+}
+
+}  // namespace pdfp

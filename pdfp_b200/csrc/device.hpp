@@ -1,0 +1,97 @@
+// device.hpp -- device memory ownership, errors, and the uploaded matrix.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "layout.hpp"
+
+namespace pdfp {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Status codes (mirror include/pdfp_b200.h).
+enum : int { E_INVALID = -1, E_CUDA = -2, E_NOMEM = -3, E_TIMEOUT = -4, E_UNSUPPORTED = -5,
+             E_NODEVICE = -6 };
+
+void set_last_error(const std::string& msg);
+
+#define PDFP_CK(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            throw ::pdfp::Error(e_ == cudaErrorMemoryAllocation ? ::pdfp::E_NOMEM                \
+                                                                : ::pdfp::E_CUDA,               \
+                                std::string(#expr) + ": " + cudaGetErrorString(e_));            \
+        }                                                                                       \
+    } while (0)
+
+// Owns device allocations; every buffer is zero-filled and padded by 64 bytes
+// so that 16-byte-rounded bulk copies of any sub-range stay inside it.
+class DeviceArena {
+  public:
+    DeviceArena() = default;
+    DeviceArena(const DeviceArena&) = delete;
+    DeviceArena& operator=(const DeviceArena&) = delete;
+    ~DeviceArena() { release(); }
+    template <class T>
+    T* alloc(size_t n) {
+        size_t bytes = ((n * sizeof(T) + 63) & ~size_t(63)) + 64;
+        void* p = nullptr;
+        PDFP_CK(cudaMalloc(&p, bytes));
+        ptrs_.push_back(p);
+        PDFP_CK(cudaMemset(p, 0, bytes));
+        bytes_ += bytes;
+        return static_cast<T*>(p);
+    }
+    template <class T>
+    T* upload(const std::vector<T>& h) {
+        T* d = alloc<T>(h.size());
+        if (!h.empty()) PDFP_CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return d;
+    }
+    void release() {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+        bytes_ = 0;
+    }
+    size_t bytes() const { return bytes_; }
+
+  private:
+    std::vector<void*> ptrs_;
+    size_t bytes_ = 0;
+};
+
+// The packed matrix of a batch on the device: A and A' in FP64 (+FP32 copies
+// when asked), index maps, and any number of tilings.
+class DeviceMatrix {
+  public:
+    HostLayout L;
+    int32_t *rp_a = nullptr, *ci_a = nullptr, *rp_t = nullptr, *ci_t = nullptr;
+    double *v64_a = nullptr, *v64_t = nullptr;
+    float *v32_a = nullptr, *v32_t = nullptr;
+    int32_t *row_off = nullptr, *col_off = nullptr, *n_eq = nullptr;
+    int32_t *row_orig = nullptr, *col_orig = nullptr;
+    int32_t max_m = 0, max_n = 0;
+
+    // Upload L (which must already be built) and, if want_f32, FP32 values.
+    void upload(DeviceArena& ar, bool want_f32);
+    // Refresh the FP32 copies from the FP64 values (after scaling on device).
+    void refresh_f32(cudaStream_t s);
+
+    struct Tiling {
+        HostTiling host;
+        SideDev dev{};
+        int32_t* inst_tile0 = nullptr;  // device copy, K + 1
+    };
+    // Build and upload a tiling of A (transpose = false) or A'.
+    Tiling make_tiling(DeviceArena& ar, bool transpose, const StageGeom& g) const;
+};
+
+}  // namespace pdfp

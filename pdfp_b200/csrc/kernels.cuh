@@ -1,0 +1,124 @@
+// kernels.cuh -- launch helpers and the small kernels around the tile engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "common.cuh"
+#include "layout.hpp"
+#include "state.hpp"
+#include "tile_spmv.cuh"
+
+namespace pdfp {
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ---- launching the tile engine ----------------------------------------------------
+
+template <class Op>
+size_t tile_dyn_smem(const SideDev& s) {
+    size_t nv = Op::NV > 0 ? Op::NV : 1;
+    return 2 * static_cast<size_t>(s.stage_bytes) +
+           ((nv * s.max_tile_rows * sizeof(typename Op::AT) + 127) & ~size_t(127));
+}
+
+// Persistent grid size for an Op on a side (blocks resident on all SMs).
+template <class Op>
+int tile_grid(const SideDev& s, int num_sms) {
+    const size_t smem = tile_dyn_smem<Op>(s);
+    cudaFuncSetAttribute(tile_spmv_kernel<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_spmv_kernel<Op>, Op::NT, smem);
+    const int per_sm = blocks > 0 ? blocks : 1;
+    int g = per_sm * num_sms;
+    return g < s.n_tiles ? g : s.n_tiles;
+}
+
+template <class Op>
+void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream) {
+    if (s.n_tiles <= 0 || grid <= 0) return;
+    tile_spmv_kernel<Op><<<grid, Op::NT, tile_dyn_smem<Op>(s), stream>>>(s, op);
+}
+
+// ---- per-tile elementwise reductions and per-instance finalisation ---------------
+// A RowsOp walks the rows of each tile of a tiling (one block per tile, one
+// thread per row), accumulating NP FP64 partial sums per tile.
+
+template <class RowsOp>
+__global__ void __launch_bounds__(256) tile_rows_kernel(const SideDev s, const RowsOp op) {
+    constexpr int NP = RowsOp::NP;
+    __shared__ double red[(NP > 0 ? NP : 1) * 8];
+    const int32_t t = blockIdx.x;
+    const int32_t inst = s.tile_inst[t];
+    if (!op.active(inst)) return;
+    const int32_t r0 = s.tile_row[t], r1 = s.tile_row[t + 1];
+    double acc[NP > 0 ? NP : 1];
+#pragma unroll
+    for (int k = 0; k < (NP > 0 ? NP : 1); ++k) acc[k] = 0.0;
+    for (int32_t r = r0 + threadIdx.x; r < r1; r += 256) op.row(r, inst, acc);
+    if (NP > 0) {
+        block_sum<256, (NP > 0 ? NP : 1)>(acc, red);
+        if (threadIdx.x == 0) op.write_partials(t, acc);
+    }
+}
+
+template <class RowsOp>
+void launch_rows(const SideDev& s, const RowsOp& op, cudaStream_t stream) {
+    if (s.n_tiles <= 0) return;
+    tile_rows_kernel<RowsOp><<<s.n_tiles, 256, 0, stream>>>(s, op);
+}
+
+// One block per instance: reduce NA partials from tiling A (tiles
+// [ta0[p], ta0[p+1])) and NB from tiling B, then op.finalize(p, sums).
+template <class FinOp>
+__global__ void __launch_bounds__(256) finalize_kernel(const FinOp op) {
+    constexpr int NA = FinOp::NA, NB = FinOp::NB, N = NA + NB;
+    __shared__ double red[N * 8];
+    const int p = blockIdx.x;
+    if (!op.active(p)) return;
+    double a[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) a[k] = 0.0;
+    if (NA > 0)
+        for (int32_t t = op.ta0[p] + threadIdx.x; t < op.ta0[p + 1]; t += 256)
+#pragma unroll
+            for (int k = 0; k < (NA > 0 ? NA : 1); ++k) a[k] += op.pa[t * (NA > 0 ? NA : 1) + k];
+    if (NB > 0)
+        for (int32_t t = op.tb0[p] + threadIdx.x; t < op.tb0[p + 1]; t += 256)
+#pragma unroll
+            for (int k = 0; k < (NB > 0 ? NB : 1); ++k) a[NA + k] += op.pb[t * (NB > 0 ? NB : 1) + k];
+    block_sum<256, N>(a, red);
+    if (threadIdx.x == 0) op.finalize(p, a);
+}
+
+template <class FinOp>
+void launch_finalize(int K, const FinOp& op, cudaStream_t stream) {
+    if (K <= 0) return;
+    finalize_kernel<FinOp><<<K, 256, 0, stream>>>(op);
+}
+
+// Per-instance elementwise kernel: blockIdx.y = instance, x strides its range.
+template <class ElemOp>
+__global__ void __launch_bounds__(256) inst_elem_kernel(const ElemOp op) {
+    const int p = blockIdx.y;
+    if (!op.active(p)) return;
+    const int32_t b = op.begin(p), e = op.end(p);
+    for (int32_t i = b + blockIdx.x * 256 + threadIdx.x; i < e; i += gridDim.x * 256) op.elem(p, i);
+}
+
+template <class ElemOp>
+void launch_elem(int K, int64_t max_len, const ElemOp& op, cudaStream_t stream) {
+    if (K <= 0 || max_len <= 0) return;
+    int64_t gx = (max_len + 255) / 256;
+    if (gx > 2048) gx = 2048;
+    dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(K));
+    inst_elem_kernel<ElemOp><<<grid, 256, 0, stream>>>(op);
+}
+
+}  // namespace pdfp

@@ -1,0 +1,854 @@
+// pdfp.cu -- the PDFP projector: PDFPState / pdfp_solve! on the device.
+//
+// Restarted Halpern PDHG with reflection on the l1-projection saddle point
+// (src/pdfp.jl:1-288, src/pdfp_kernels.jl:1-86), for a batch of instances
+// packed block-diagonally in one handle.  One evaluation window (the
+// reference's `freq` steps followed by compute_fixed_point_error!,
+// compute_residual!, should_restart and perform_restart!, src/pdfp.jl:258-285)
+// is a fixed launch sequence captured once as a CUDA graph; every decision in
+// it is taken on the device from the per-instance state, so the host only
+// replays the graph and polls one status word per instance per window.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+
+#include "../../include/pdfp_b200.h"
+#include "device.hpp"
+#include "kernels.cuh"
+#include "pdfp_ops.cuh"
+#include "power.cuh"
+#include "projector.hpp"
+
+namespace pdfp {
+
+constexpr int NT_ITER = 512;
+constexpr int NT_EVAL = 256;
+constexpr int STALL_EVALS = 10;  // evaluations without 10% KKT progress before the FP64 polish
+
+// ---- per-instance state kernels ---------------------------------------------------
+
+__global__ void solve_begin_kernel(InstState* st, int K) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < K) st[p].t_start_ns = globaltimer_ns();
+}
+
+__global__ void set_max_sv_kernel(InstState* st, const double* sv, int K) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < K && !isnan(sv[p])) st[p].max_sv = sv[p];
+}
+
+// initialize_step_size_and_primal_weight! (src/pdfp.jl:220-241) minus the two
+// denominators, plus this solve's parameters.
+__global__ void solve_init_kernel(InstState* st, InstFlags* fl, const SolveParams* sp, int K) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= K) return;
+    InstState& s = st[p];
+    const SolveParams& q = sp[p];
+    s.eps_opt = q.eps_opt;
+    s.eps_feas = q.eps_feas;
+    s.time_limit = q.time_limit;
+    s.iter_limit = q.iter_limit;
+    s.freq = q.freq;
+    s.omega = q.omega;
+    s.art = q.art;
+    s.suff = q.suff;
+    s.nec = q.nec;
+    s.kp = q.kp;
+    s.ki = q.ki;
+    s.kd = q.kd;
+    s.ismooth = q.ismooth;
+    s.step_size = s.nnz_zero ? 1.0 : 0.998 / sqrt(1.0 + s.max_sv * s.max_sv);
+    s.primal_weight = q.primal_weight;
+    s.best_primal_weight = q.primal_weight;
+    s.err_sum = 0.0;
+    s.last_err = 0.0;
+    s.tau = s.step_size / s.primal_weight;
+    s.sigma = s.step_size * s.primal_weight;
+    s.mode = q.mode;
+    s.best_score = INFINITY;
+    s.stall = 0;
+    s.polish_windows = 0;
+    s.do_restart = 0;
+    s.restart_now = 0;
+    s.restarts = 0;
+    s.status = s.total < q.iter_limit ? ST_RUNNING : ST_ITERATION_LIMIT;
+    fl[p] = InstFlags{s.status, s.mode, 0, 0};
+}
+
+// warm_start! (src/pdfp.jl:104-114): the counter part.
+__global__ void warm_start_state_kernel(InstState* st, int p) {
+    InstState& s = st[p];
+    s.inner = 0;
+    s.total = 0;
+    s.fpe = INFINITY;
+    s.last_trial_fpe = INFINITY;
+    s.status = ST_RUNNING;
+}
+
+// ---- denominators of the relative residuals (src/pdfp.jl:236-239) -----------------
+
+struct DenRows {
+    static constexpr int NP = 2;
+    const double *w, *xt;
+    double* part;
+    __device__ bool active(int) const { return true; }
+    __device__ void row(int32_t j, int, double* acc) const {
+        const double w_ = w[j];
+        if (w_ >= 0.0) {
+            acc[0] += w_ * w_;
+            acc[1] += mul_rn(w_, fabs(xt[j]));
+        }
+    }
+    __device__ void write_partials(int32_t t, const double* acc) const {
+        part[t * 8] = acc[0];
+        part[t * 8 + 1] = acc[1];
+#pragma unroll
+        for (int k = 2; k < 8; ++k) part[t * 8 + k] = 0.0;
+    }
+};
+
+struct DenFin {
+    static constexpr int NA = 8, NB = 0;
+    const int32_t* ta0;
+    const double* pa;
+    const int32_t* tb0;
+    const double* pb;
+    InstState* st;
+    __device__ bool active(int) const { return true; }
+    __device__ void finalize(int p, const double* a) const {
+        st[p].dual_den = 1.0 + sqrt(a[0]);
+        st[p].gap_den = 1.0 + a[1];
+    }
+};
+
+// ---- the controller: restart and termination rules on the device --------------
+
+// should_restart, src/pdlp.jl:167-181
+__device__ bool should_restart(InstState& s) {
+    bool restart = false;
+    const int64_t freq = s.freq;
+    if (s.total == freq) {
+        restart = true;
+    } else if (s.total > freq) {
+        if (s.fpe <= s.suff * s.initial_fpe) restart = true;
+        if (s.fpe <= s.nec * s.initial_fpe && s.fpe > s.last_trial_fpe) restart = true;
+        if (static_cast<double>(s.inner) >= s.art * static_cast<double>(s.total)) restart = true;
+    }
+    s.last_trial_fpe = s.fpe;
+    return restart;
+}
+
+// update_primal_weight!, src/pdlp.jl:185-205
+__device__ void update_primal_weight(InstState& s, double primal_dist, double dual_dist) {
+    const double eps = 2.220446049250313e-16;
+    const double ratio = s.rel_d / jl_max(s.rel_p, eps);
+    if (1e-16 < primal_dist && primal_dist < 1e12 && 1e-16 < dual_dist && dual_dist < 1e12 &&
+        1e-8 < ratio && ratio < 1e8) {
+        const double err = log(dual_dist) - log(primal_dist) - log(s.primal_weight);
+        s.err_sum *= s.ismooth;
+        s.err_sum += err;
+        const double delta_err = err - s.last_err;
+        s.primal_weight *= exp(s.kp * err + s.ki * s.err_sum + s.kd * delta_err);
+        s.last_err = err;
+    } else {
+        s.primal_weight = s.best_primal_weight;
+        s.err_sum = 0.0;
+        s.last_err = 0.0;
+    }
+    const double gap = fabs(log10(s.rel_d / jl_max(s.rel_p, eps)));
+    if (gap < s.best_gap) {
+        s.best_gap = gap;
+        s.best_primal_weight = s.primal_weight;
+    }
+}
+
+enum : int32_t { PHASE_AFTER_FIRST = 0, PHASE_EVAL = 1 };
+
+struct Controller {
+    static constexpr int NA = 8, NB = 4;
+    const int32_t* ta0;
+    const double* pa;
+    const int32_t* tb0;
+    const double* pb;
+    InstState* st;
+    InstFlags* fl;
+    int32_t phase, polish;
+    __device__ bool active(int p) const {
+        return st[p].status == ST_RUNNING && (phase == PHASE_EVAL || st[p].do_restart);
+    }
+    __device__ void finalize(int p, const double* a) const {
+        InstState& s = st[p];
+        const double pw = s.primal_weight;
+        // compute_fixed_point_error!, src/pdfp.jl:171-176
+        const double movement = a[0] * pw + (a[1] + a[10]) / pw;
+        const double interaction = 2.0 * s.step_size * a[2];
+        const double fpe = sqrt(jl_max(movement + interaction, 0.0));
+        s.fpe = fpe;
+        if (phase == PHASE_AFTER_FIRST) {  // src/pdfp.jl:260-264
+            s.initial_fpe = fpe;
+            s.do_restart = 0;
+            return;
+        }
+        // compute_residual!, src/pdfp.jl:200-218
+        s.rel_p = sqrt(a[8]) / (1.0 + s.b_norm);
+        s.rel_d = sqrt(a[3]) / s.dual_den;
+        s.l1 = a[4];
+        s.rel_gap = fabs(a[5] + a[9] - a[4]) / s.gap_den;
+        s.inner += s.freq;
+        s.total += s.freq;
+        s.restart_now = 0;
+        int32_t request = 0;
+        if (s.rel_p <= s.eps_feas && s.rel_d <= s.eps_opt && s.rel_gap <= s.eps_opt) {
+            s.status = ST_OPTIMAL;
+        } else if (static_cast<double>(globaltimer_ns() - s.t_start_ns) * 1e-9 > s.time_limit) {
+            s.status = ST_TIME_LIMIT;
+        } else {
+            if (should_restart(s)) {  // perform_restart!, src/pdfp.jl:180-192
+                update_primal_weight(s, sqrt(a[6]), sqrt(a[7] + a[11]));
+                s.inner = 0;
+                s.last_trial_fpe = INFINITY;
+                s.restarts += 1;
+                s.restart_now = 1;
+                s.do_restart = 1;
+            }
+            s.tau = s.step_size / s.primal_weight;
+            s.sigma = s.step_size * s.primal_weight;
+            if (s.total >= s.iter_limit) s.status = ST_ITERATION_LIMIT;
+            if (s.status == ST_RUNNING && s.mode == MODE_FP32 && polish) {
+                // FP32 progress test: switch this instance to the FP64 form when
+                // its KKT score has not improved by 10% over STALL_EVALS evaluations.
+                const double score = fmax(s.rel_p / s.eps_feas, fmax(s.rel_d / s.eps_opt, s.rel_gap / s.eps_opt));
+                if (score < 0.9 * s.best_score) {
+                    s.best_score = score;
+                    s.stall = 0;
+                } else {
+                    s.stall += 1;
+                }
+                if (s.stall >= STALL_EVALS && score > 1.0) request = 1;
+            }
+        }
+        fl[p] = InstFlags{s.status, s.mode, request, 0};
+    }
+};
+
+// ---- vector kernels ------------------------------------------------------------------
+
+template <typename T>
+struct RestartCopy {  // perform_restart!: initial = current = pdhg (src/pdfp.jl:186-188)
+    IterVecs<T> v;
+    const InstState* st;
+    const int32_t *col_off, *row_off;
+    int32_t mode;
+    __device__ bool active(int p) const { return st[p].restart_now && st[p].mode == mode; }
+    __device__ int32_t begin(int) const { return 0; }
+    __device__ int32_t end(int p) const {
+        return (col_off[p + 1] - col_off[p]) + (row_off[p + 1] - row_off[p]);
+    }
+    __device__ void elem(int p, int32_t i) const {
+        const int32_t n = col_off[p + 1] - col_off[p];
+        if (i < n) {
+            const int32_t j = col_off[p] + i;
+            const T x = v.px[j], y = v.py[j];
+            v.ix[j] = x; v.cx[j] = x;
+            v.iy[j] = y; v.cy[j] = y;
+        } else {
+            const int32_t r = row_off[p] + (i - n);
+            const T z = v.pz[r];
+            v.iz[r] = z; v.cz[r] = z;
+        }
+    }
+};
+
+template <typename T>
+struct WarmStartCopy {  // initial = current (src/pdfp.jl:105-107)
+    IterVecs<T> v;
+    const int32_t *col_off, *row_off;
+    int32_t only;
+    __device__ bool active(int p) const { return p == only; }
+    __device__ int32_t begin(int) const { return 0; }
+    __device__ int32_t end(int p) const {
+        return (col_off[p + 1] - col_off[p]) + (row_off[p + 1] - row_off[p]);
+    }
+    __device__ void elem(int p, int32_t i) const {
+        const int32_t n = col_off[p + 1] - col_off[p];
+        if (i < n) {
+            const int32_t j = col_off[p] + i;
+            v.ix[j] = v.cx[j];
+            v.iy[j] = v.cy[j];
+        } else {
+            const int32_t r = row_off[p] + (i - n);
+            v.iz[r] = v.cz[r];
+        }
+    }
+};
+
+// dst[packed j] = src[caller index of j] for instance `only` (columns or rows)
+template <typename T>
+struct PermuteIn {
+    T* dst;
+    T* dst2;  // optional second destination
+    const double* src;
+    const int32_t *off, *orig;
+    int32_t only;
+    __device__ bool active(int p) const { return p == only; }
+    __device__ int32_t begin(int p) const { return off[p]; }
+    __device__ int32_t end(int p) const { return off[p + 1]; }
+    __device__ void elem(int, int32_t j) const {
+        const T x = static_cast<T>(src[orig[j]]);
+        dst[j] = x;
+        if (dst2) dst2[j] = x;
+    }
+};
+
+template <typename T>
+struct PermuteOut {
+    double* dst;
+    const T* src;
+    const int32_t *off, *orig;
+    int32_t only;
+    __device__ bool active(int p) const { return p == only; }
+    __device__ int32_t begin(int p) const { return off[p]; }
+    __device__ int32_t end(int p) const { return off[p + 1]; }
+    __device__ void elem(int, int32_t j) const { dst[orig[j]] = static_cast<double>(src[j]); }
+};
+
+template <typename S, typename D>
+struct ConvertVecs {  // the live iterate set of instance `only`: S -> D
+    IterVecs<S> s;
+    IterVecs<D> d;
+    const int32_t *col_off, *row_off;
+    int32_t only;
+    __device__ bool active(int p) const { return p == only; }
+    __device__ int32_t begin(int) const { return 0; }
+    __device__ int32_t end(int p) const {
+        return (col_off[p + 1] - col_off[p]) + (row_off[p + 1] - row_off[p]);
+    }
+    __device__ void elem(int p, int32_t i) const {
+        const int32_t n = col_off[p + 1] - col_off[p];
+        if (i < n) {
+            const int32_t j = col_off[p] + i;
+            d.cx[j] = static_cast<D>(s.cx[j]); d.ix[j] = static_cast<D>(s.ix[j]);
+            d.px[j] = static_cast<D>(s.px[j]); d.rx[j] = static_cast<D>(s.rx[j]);
+            d.cy[j] = static_cast<D>(s.cy[j]); d.iy[j] = static_cast<D>(s.iy[j]);
+            d.py[j] = static_cast<D>(s.py[j]); d.ry[j] = static_cast<D>(s.ry[j]);
+            d.ds[j] = static_cast<D>(s.ds[j]);
+        } else {
+            const int32_t r = row_off[p] + (i - n);
+            d.cz[r] = static_cast<D>(s.cz[r]); d.iz[r] = static_cast<D>(s.iz[r]);
+            d.pz[r] = static_cast<D>(s.pz[r]); d.rz[r] = static_cast<D>(s.rz[r]);
+        }
+    }
+};
+
+__global__ void set_mode_kernel(InstState* st, int p, int32_t mode) { st[p].mode = mode; }
+
+// Save every instance's status and mark it running (timing runs), or restore it.
+__global__ void swap_status_kernel(InstState* st, int32_t* saved, int K, int restore) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= K) return;
+    if (restore) {
+        st[p].status = saved[p];
+    } else {
+        saved[p] = st[p].status;
+        st[p].status = ST_RUNNING;
+    }
+}
+
+// ---- the projector ----------------------------------------------------------------------
+
+template <typename T>
+static IterVecs<T> alloc_vecs(DeviceArena& ar, int64_t N, int64_t M) {
+    IterVecs<T> v{};
+    T** nv[] = {&v.cx, &v.ix, &v.px, &v.rx, &v.cy, &v.iy, &v.py, &v.ry, &v.ds, &v.lb, &v.ub, &v.xt, &v.w};
+    for (T** q : nv) *q = ar.alloc<T>(N);
+    T** mv[] = {&v.cz, &v.iz, &v.pz, &v.rz, &v.b};
+    for (T** q : mv) *q = ar.alloc<T>(M);
+    return v;
+}
+
+Projector::Projector(const std::vector<ProblemData>& probs, int precision) : precision_(precision) {
+    int dev = 0;
+    PDFP_CK(cudaGetDevice(&dev));
+    PDFP_CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+    PDFP_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    std::vector<ProblemIn> in;
+    for (const ProblemData& p : probs)
+        in.push_back(ProblemIn{p.m, p.n, p.rp, p.ci, p.v, p.is_eq});
+    std::string msg = build_layout(in, true, M_.L);
+    if (!msg.empty()) throw Error(E_INVALID, msg);
+    const HostLayout& L = M_.L;
+    K_ = L.K;
+    M_.upload(ar_, precision_ == PDFP_MIXED);
+
+    // tilings
+    StageGeom git{precision_ == PDFP_MIXED ? 4 : 8, precision_ == PDFP_MIXED ? 4 : 8,
+                  precision_ == PDFP_MIXED ? 4 : 8, 8, 1, 40 * 1024, 2048};
+    it_t_ = M_.make_tiling(ar_, true, git);
+    git.nvec = 3;
+    it_a_ = M_.make_tiling(ar_, false, git);
+    if (precision_ == PDFP_MIXED) {  // FP64 tilings for the polish
+        StageGeom g64{8, 8, 8, 8, 1, 40 * 1024, 2048};
+        it64_t_ = M_.make_tiling(ar_, true, g64);
+        g64.nvec = 3;
+        it64_a_ = M_.make_tiling(ar_, false, g64);
+    }
+    StageGeom gev{8, 8, 8, 0, 2, 32 * 1024, 2048};
+    ev_t_ = M_.make_tiling(ar_, true, gev);
+    ev_a_ = M_.make_tiling(ar_, false, gev);
+
+    // vectors
+    v64_ = alloc_vecs<double>(ar_, L.N, L.M);
+    v64_.val_t = M_.v64_t;
+    v64_.val_a = M_.v64_a;
+    if (precision_ == PDFP_MIXED) {
+        v32_ = alloc_vecs<float>(ar_, L.N, L.M);
+        v32_.val_t = M_.v32_t;
+        v32_.val_a = M_.v32_a;
+    }
+    row_unscale_ = nullptr;
+    part_col_ = ar_.alloc<double>(8 * static_cast<size_t>(std::max(ev_t_.dev.n_tiles, 1)));
+    part_row_ = ar_.alloc<double>(4 * static_cast<size_t>(std::max(ev_a_.dev.n_tiles, 1)));
+    st_ = ar_.alloc<InstState>(K_);
+    flags_ = ar_.alloc<InstFlags>(K_ + 1);
+    err_ = ar_.alloc<int32_t>(4);
+    sp_ = ar_.alloc<SolveParams>(K_);
+    stage_ = ar_.alloc<double>(std::max<int64_t>(std::max(M_.max_m, M_.max_n), 1));
+    PDFP_CK(cudaMallocHost(&flags_h_, sizeof(InstFlags) * (K_ + 1)));
+    vec_mode_.assign(K_, precision_ == PDFP_MIXED ? MODE_FP32 : MODE_FP64);
+
+    // per-instance data vectors (permuted into packed order)
+    bool any_unscale = false;
+    for (const ProblemData& p : probs) any_unscale = any_unscale || p.row_unscale;
+    if (any_unscale) row_unscale_ = ar_.alloc<double>(L.M);
+    std::vector<InstState> hs(K_);
+    std::vector<double> hb(L.M), hlb(L.N), hub(L.N), hw(L.N), hru(any_unscale ? L.M : 0);
+    for (int p = 0; p < K_; ++p) {
+        const ProblemData& P = probs[p];
+        const int32_t c0 = L.col_off[p], r0 = L.row_off[p];
+        for (int32_t j = 0; j < P.n; ++j) {
+            const int32_t o = L.col_orig[c0 + j];
+            if (std::isnan(P.lb[o]) || std::isnan(P.ub[o]) || std::isnan(P.w[o]))
+                throw Error(E_INVALID, "NaN in var_lb, var_ub or w");
+            hlb[c0 + j] = P.lb[o];
+            hub[c0 + j] = P.ub[o];
+            hw[c0 + j] = P.is_int[o] ? std::fabs(P.w[o]) : -1.0;
+        }
+        double bsq = 0.0, bosq = 0.0;
+        for (int32_t i = 0; i < P.m; ++i) {
+            const int32_t o = L.row_orig[r0 + i];
+            if (!std::isfinite(P.b[o])) throw Error(E_INVALID, "non-finite right-hand side");
+            hb[r0 + i] = P.b[o];
+            bsq += P.b[o] * P.b[o];
+            if (P.row_unscale) {
+                hru[r0 + i] = P.row_unscale[o];
+                const double t = P.b[o] * P.row_unscale[o];  // b ./ D_r  (src/pdfp.jl:87)
+                bosq += t * t;
+            } else if (any_unscale) {
+                hru[r0 + i] = 1.0;
+            }
+        }
+        InstState& s = hs[p];
+        std::memset(&s, 0, sizeof(s));
+        s.max_sv = NAN;
+        s.primal_weight = 1.0;
+        s.best_primal_weight = 1.0;
+        s.best_gap = INFINITY;
+        s.fpe = INFINITY;
+        s.initial_fpe = INFINITY;
+        s.last_trial_fpe = INFINITY;
+        s.rel_p = s.rel_d = s.rel_gap = INFINITY;
+        s.dual_den = 1.0;
+        s.gap_den = 1.0;
+        s.b_norm = P.row_unscale ? std::sqrt(bosq) : std::sqrt(bsq);
+        s.nnz_zero = (P.m == 0 || P.rp[P.m] == 0) ? 1 : 0;
+        s.mode = vec_mode_[p];
+        s.status = ST_RUNNING;
+        has_unscale_.push_back(P.row_unscale != nullptr);
+    }
+    auto up = [&](double* d, const std::vector<double>& h) {
+        if (!h.empty()) PDFP_CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    };
+    up(v64_.b, hb);
+    up(v64_.lb, hlb);
+    up(v64_.ub, hub);
+    up(v64_.w, hw);
+    if (any_unscale) up(row_unscale_, hru);
+    if (precision_ == PDFP_MIXED) {
+        auto cast = [&](float* d, const std::vector<double>& h) {
+            std::vector<float> f(h.size());
+            for (size_t i = 0; i < h.size(); ++i) f[i] = static_cast<float>(h[i]);
+            if (!f.empty()) PDFP_CK(cudaMemcpy(d, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+        };
+        cast(v32_.b, hb);
+        cast(v32_.lb, hlb);
+        cast(v32_.ub, hub);
+        cast(v32_.w, hw);
+    }
+    PDFP_CK(cudaMemcpy(st_, hs.data(), sizeof(InstState) * K_, cudaMemcpyHostToDevice));
+
+    ed_.xt = v64_.xt;
+    ed_.w = v64_.w;
+    ed_.b = v64_.b;
+    ed_.row_unscale = row_unscale_;
+    ed_.val_t = M_.v64_t;
+    ed_.val_a = M_.v64_a;
+    ed_.part_col = part_col_;
+    ed_.part_row = part_row_;
+    PDFP_CK(cudaDeviceSynchronize());
+}
+
+Projector::~Projector() {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    if (flags_h_) cudaFreeHost(flags_h_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Projector::check_instance(int p) const {
+    if (p < 0 || p >= K_) throw Error(E_INVALID, "instance index out of range");
+}
+
+void Projector::set_x(int p, const double* x) {
+    check_instance(p);
+    const HostLayout& L = M_.L;
+    const int32_t n = L.col_off[p + 1] - L.col_off[p];
+    if (n == 0) return;
+    PDFP_CK(cudaMemcpyAsync(stage_, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    if (vec_mode_[p] == MODE_FP32)
+        launch_elem(K_, n, PermuteIn<float>{v32_.cx, v32_.ix, stage_, M_.col_off, M_.col_orig, p}, stream_);
+    else
+        launch_elem(K_, n, PermuteIn<double>{v64_.cx, v64_.ix, stage_, M_.col_off, M_.col_orig, p}, stream_);
+    PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaStreamSynchronize(stream_));
+}
+
+void Projector::set_target(int p, const double* xt) {
+    check_instance(p);
+    const HostLayout& L = M_.L;
+    const int32_t n = L.col_off[p + 1] - L.col_off[p];
+    if (n > 0) {
+        for (int32_t j = 0; j < n; ++j)
+            if (std::isnan(xt[j])) throw Error(E_INVALID, "NaN in the target");
+        PDFP_CK(cudaMemcpyAsync(stage_, xt, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+        launch_elem(K_, n, PermuteIn<double>{v64_.xt, nullptr, stage_, M_.col_off, M_.col_orig, p}, stream_);
+        if (precision_ == PDFP_MIXED)
+            launch_elem(K_, n, PermuteIn<float>{v32_.xt, nullptr, stage_, M_.col_off, M_.col_orig, p}, stream_);
+        PDFP_CK(cudaGetLastError());
+    }
+    warm_start(p);
+}
+
+void Projector::warm_start(int p) {
+    check_instance(p);
+    const HostLayout& L = M_.L;
+    const int64_t len = (L.col_off[p + 1] - L.col_off[p]) + (L.row_off[p + 1] - L.row_off[p]);
+    if (vec_mode_[p] == MODE_FP32)
+        launch_elem(K_, len, WarmStartCopy<float>{v32_, M_.col_off, M_.row_off, p}, stream_);
+    else
+        launch_elem(K_, len, WarmStartCopy<double>{v64_, M_.col_off, M_.row_off, p}, stream_);
+    warm_start_state_kernel<<<1, 1, 0, stream_>>>(st_, p);
+    PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaStreamSynchronize(stream_));
+}
+
+void Projector::get_vector(int p, int which, double* out) {
+    check_instance(p);
+    const HostLayout& L = M_.L;
+    const bool rowvec = (which == PDFP_VEC_PDHG_Z || which == PDFP_VEC_CURRENT_Z);
+    const int32_t len = rowvec ? L.row_off[p + 1] - L.row_off[p] : L.col_off[p + 1] - L.col_off[p];
+    if (len == 0) return;
+    auto pick = [&](auto& v) -> decltype(v.px) {
+        switch (which) {
+            case PDFP_VEC_PDHG_X: return v.px;
+            case PDFP_VEC_PDHG_Y: return v.py;
+            case PDFP_VEC_PDHG_Z: return v.pz;
+            case PDFP_VEC_CURRENT_X: return v.cx;
+            case PDFP_VEC_CURRENT_Y: return v.cy;
+            case PDFP_VEC_CURRENT_Z: return v.cz;
+            case PDFP_VEC_DUAL_SLACK: return v.ds;
+            case PDFP_VEC_REFLECTED_X: return v.rx;
+            default: throw Error(E_INVALID, "unknown vector");
+        }
+    };
+    const int32_t* off = rowvec ? M_.row_off : M_.col_off;
+    const int32_t* orig = rowvec ? M_.row_orig : M_.col_orig;
+    if (vec_mode_[p] == MODE_FP32)
+        launch_elem(K_, len, PermuteOut<float>{stage_, pick(v32_), off, orig, p}, stream_);
+    else
+        launch_elem(K_, len, PermuteOut<double>{stage_, pick(v64_), off, orig, p}, stream_);
+    PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaMemcpyAsync(out, stage_, sizeof(double) * len, cudaMemcpyDeviceToHost, stream_));
+    PDFP_CK(cudaStreamSynchronize(stream_));
+}
+
+void Projector::ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance) {
+    std::vector<InstState> hs(K_);
+    PDFP_CK(cudaMemcpy(hs.data(), st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost));
+    std::vector<int> run(K_, 0);
+    bool any = false;
+    for (int p = 0; p < K_; ++p) {
+        run[p] = (!hs[p].nnz_zero && std::isnan(hs[p].max_sv)) ? 1 : 0;  // cached per run (src/pdfp.jl:225-229)
+        any = any || run[p];
+    }
+    if (!any) return;
+    std::vector<double> sv = power_iteration(M_, ar_, ev_a_, ev_t_, run, sv_max_iterations,
+                                             sv_tolerance, stream_, num_sms_, err_, nullptr);
+    DeviceArena tmp;
+    double* d = tmp.alloc<double>(K_);
+    PDFP_CK(cudaMemcpy(d, sv.data(), sizeof(double) * K_, cudaMemcpyHostToDevice));
+    set_max_sv_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, d, K_);
+    PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaStreamSynchronize(stream_));
+}
+
+void Projector::record_window(int freq, bool with32, bool with64) {
+    const int mode32 = MODE_FP32, mode64 = MODE_FP64;
+    auto prim32 = [&](int k, bool major) {
+        if (major)
+            launch_tile(it_t_.dev, PrimalOp<float, true, NT_ITER>{v32_, st_, k, mode32, err_}, g_.p32, stream_);
+        else
+            launch_tile(it_t_.dev, PrimalOp<float, false, NT_ITER>{v32_, st_, k, mode32, err_}, g_.p32, stream_);
+    };
+    auto dual32 = [&](int k, bool major) {
+        if (major)
+            launch_tile(it_a_.dev, DualOp<float, true, NT_ITER>{v32_, st_, M_.row_off, M_.n_eq, k, mode32, err_}, g_.d32, stream_);
+        else
+            launch_tile(it_a_.dev, DualOp<float, false, NT_ITER>{v32_, st_, M_.row_off, M_.n_eq, k, mode32, err_}, g_.d32, stream_);
+    };
+    const DeviceMatrix::Tiling& t64 = precision_ == PDFP_MIXED ? it64_t_ : it_t_;
+    const DeviceMatrix::Tiling& a64 = precision_ == PDFP_MIXED ? it64_a_ : it_a_;
+    auto prim64 = [&](int k, bool major) {
+        if (major)
+            launch_tile(t64.dev, PrimalOp<double, true, NT_ITER>{v64_, st_, k, mode64, err_}, g_.p64, stream_);
+        else
+            launch_tile(t64.dev, PrimalOp<double, false, NT_ITER>{v64_, st_, k, mode64, err_}, g_.p64, stream_);
+    };
+    auto dual64 = [&](int k, bool major) {
+        if (major)
+            launch_tile(a64.dev, DualOp<double, true, NT_ITER>{v64_, st_, M_.row_off, M_.n_eq, k, mode64, err_}, g_.d64, stream_);
+        else
+            launch_tile(a64.dev, DualOp<double, false, NT_ITER>{v64_, st_, M_.row_off, M_.n_eq, k, mode64, err_}, g_.d64, stream_);
+    };
+    auto evals = [&](int which) {
+        if (with32) {
+            launch_tile(ev_t_.dev, EvalColOp<float, NT_EVAL>{v32_, ed_, st_, which, mode32, err_}, g_.ec, stream_);
+            launch_tile(ev_a_.dev, EvalRowOp<float, NT_EVAL>{v32_, ed_, st_, M_.row_off, M_.n_eq, which, mode32, err_}, g_.er, stream_);
+        }
+        if (with64) {
+            launch_tile(ev_t_.dev, EvalColOp<double, NT_EVAL>{v64_, ed_, st_, which, mode64, err_}, g_.ec, stream_);
+            launch_tile(ev_a_.dev, EvalRowOp<double, NT_EVAL>{v64_, ed_, st_, M_.row_off, M_.n_eq, which, mode64, err_}, g_.er, stream_);
+        }
+    };
+    for (int i = 1; i <= freq; ++i) {
+        const bool major = (i == 1 || i == freq);
+        if (with32) { prim32(i, major); dual32(i, major); }
+        if (with64) { prim64(i, major); dual64(i, major); }
+        if (i == 1) {
+            evals(EVAL_AFTER_RESTART);
+            launch_finalize(K_, Controller{ev_t_.inst_tile0, part_col_, ev_a_.inst_tile0, part_row_, st_, flags_, PHASE_AFTER_FIRST, polish_enabled_}, stream_);
+        }
+    }
+    evals(EVAL_FULL);
+    launch_finalize(K_, Controller{ev_t_.inst_tile0, part_col_, ev_a_.inst_tile0, part_row_, st_, flags_, PHASE_EVAL, polish_enabled_}, stream_);
+    const int64_t maxlen = static_cast<int64_t>(M_.max_m) + M_.max_n;
+    if (with32) launch_elem(K_, maxlen, RestartCopy<float>{v32_, st_, M_.col_off, M_.row_off, mode32}, stream_);
+    if (with64) launch_elem(K_, maxlen, RestartCopy<double>{v64_, st_, M_.col_off, M_.row_off, mode64}, stream_);
+}
+
+cudaGraphExec_t Projector::window_graph(int freq, bool with32, bool with64) {
+    const int key = freq * 4 + (with32 ? 1 : 0) + (with64 ? 2 : 0);
+    auto it = graphs_.find(key);
+    if (it != graphs_.end()) return it->second;
+    // persistent grid sizes (outside capture)
+    g_.p32 = precision_ == PDFP_MIXED ? tile_grid<PrimalOp<float, true, NT_ITER>>(it_t_.dev, num_sms_) : 0;
+    g_.d32 = precision_ == PDFP_MIXED ? tile_grid<DualOp<float, true, NT_ITER>>(it_a_.dev, num_sms_) : 0;
+    {
+        const DeviceMatrix::Tiling& t64 = precision_ == PDFP_MIXED ? it64_t_ : it_t_;
+        const DeviceMatrix::Tiling& a64 = precision_ == PDFP_MIXED ? it64_a_ : it_a_;
+        g_.p64 = tile_grid<PrimalOp<double, true, NT_ITER>>(t64.dev, num_sms_);
+        g_.d64 = tile_grid<DualOp<double, true, NT_ITER>>(a64.dev, num_sms_);
+        tile_grid<PrimalOp<double, false, NT_ITER>>(t64.dev, num_sms_);
+        tile_grid<DualOp<double, false, NT_ITER>>(a64.dev, num_sms_);
+    }
+    if (precision_ == PDFP_MIXED) {
+        tile_grid<PrimalOp<float, false, NT_ITER>>(it_t_.dev, num_sms_);
+        tile_grid<DualOp<float, false, NT_ITER>>(it_a_.dev, num_sms_);
+        tile_grid<EvalColOp<float, NT_EVAL>>(ev_t_.dev, num_sms_);
+        tile_grid<EvalRowOp<float, NT_EVAL>>(ev_a_.dev, num_sms_);
+    }
+    g_.ec = tile_grid<EvalColOp<double, NT_EVAL>>(ev_t_.dev, num_sms_);
+    g_.er = tile_grid<EvalRowOp<double, NT_EVAL>>(ev_a_.dev, num_sms_);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    PDFP_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    record_window(freq, with32, with64);
+    cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+    if (e != cudaSuccess) throw Error(E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    PDFP_CK(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    graphs_[key] = exec;
+    return exec;
+}
+
+void Projector::solve(const pdfp_params* params, const double* primal_weights, pdfp_result* results) {
+    auto wall0 = std::chrono::steady_clock::now();
+    // validate and stage the parameters
+    std::vector<SolveParams> sp(K_);
+    int freq = -1;
+    int32_t sv_it = 5000;
+    double sv_tol = 1e-4;
+    double max_time = 0.0;
+    for (int p = 0; p < K_; ++p) {
+        const pdfp_params& q = params[p];
+        if (q.termination_evaluation_frequency < 1)
+            throw Error(E_INVALID, "termination_evaluation_frequency must be >= 1");
+        if (freq < 0) freq = q.termination_evaluation_frequency;
+        if (q.termination_evaluation_frequency != freq)
+            throw Error(E_INVALID, "batch members must share termination_evaluation_frequency");
+        if (!(primal_weights[p] > 0.0) || !std::isfinite(primal_weights[p]))
+            throw Error(E_INVALID, "primal_weight must be positive and finite");
+        SolveParams& s = sp[p];
+        s.eps_opt = q.eps_optimal_relative;
+        s.eps_feas = q.eps_feasible_relative;
+        s.time_limit = q.time_limit;
+        s.omega = q.reflection_coefficient;
+        s.art = q.artificial_restart_threshold;
+        s.suff = q.sufficient_reduction_for_restart;
+        s.nec = q.necessary_reduction_for_restart;
+        s.kp = q.k_p;
+        s.ki = q.k_i;
+        s.kd = q.k_d;
+        s.ismooth = q.i_smooth;
+        s.primal_weight = primal_weights[p];
+        s.iter_limit = q.iteration_limit;
+        s.freq = q.termination_evaluation_frequency;
+        s.mode = precision_ == PDFP_MIXED ? MODE_FP32 : MODE_FP64;
+        sv_it = q.sv_max_iterations;
+        sv_tol = q.sv_tolerance;
+        max_time = std::max(max_time, q.time_limit);
+    }
+    solve_begin_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, K_);
+    PDFP_CK(cudaGetLastError());
+    ensure_step_sizes(sv_it, sv_tol);
+    // a mixed handle starts every solve in FP32: bring back instances a polish left in FP64
+    if (precision_ == PDFP_MIXED) {
+        const HostLayout& L = M_.L;
+        for (int p = 0; p < K_; ++p) {
+            if (vec_mode_[p] != MODE_FP64) continue;
+            const int64_t len = (L.col_off[p + 1] - L.col_off[p]) + (L.row_off[p + 1] - L.row_off[p]);
+            launch_elem(K_, len, ConvertVecs<double, float>{v64_, v32_, M_.col_off, M_.row_off, p}, stream_);
+            vec_mode_[p] = MODE_FP32;
+        }
+    }
+    PDFP_CK(cudaMemcpyAsync(sp_, sp.data(), sizeof(SolveParams) * K_, cudaMemcpyHostToDevice, stream_));
+    solve_init_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, flags_, sp_, K_);
+    launch_rows(ev_t_.dev, DenRows{v64_.w, v64_.xt, part_col_}, stream_);
+    launch_finalize(K_, DenFin{ev_t_.inst_tile0, part_col_, nullptr, nullptr, st_}, stream_);
+    PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaMemsetAsync(err_, 0, sizeof(int32_t) * 4, stream_));
+
+    bool with32 = precision_ == PDFP_MIXED;
+    bool with64 = precision_ != PDFP_MIXED;
+    // first poll: instances may already be done (iteration_limit <= total)
+    PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
+    PDFP_CK(cudaStreamSynchronize(stream_));
+    int32_t dev_err = 0;
+    for (;;) {
+        bool running = false;
+        for (int p = 0; p < K_; ++p) running = running || flags_h_[p].status == ST_RUNNING;
+        if (!running) break;
+        cudaGraphExec_t g = window_graph(freq, with32, with64);
+        PDFP_CK(cudaGraphLaunch(g, stream_));
+        PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
+        PDFP_CK(cudaMemcpyAsync(&flags_h_[K_].status, err_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+        PDFP_CK(cudaStreamSynchronize(stream_));
+        dev_err = flags_h_[K_].status;
+        if (dev_err) throw Error(E_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+        // FP64 polish for instances whose FP32 progress stalled
+        for (int p = 0; p < K_; ++p) {
+            if (flags_h_[p].polish_request && flags_h_[p].status == ST_RUNNING && vec_mode_[p] == MODE_FP32) {
+                const HostLayout& L = M_.L;
+                const int64_t len = (L.col_off[p + 1] - L.col_off[p]) + (L.row_off[p + 1] - L.row_off[p]);
+                launch_elem(K_, len, ConvertVecs<float, double>{v32_, v64_, M_.col_off, M_.row_off, p}, stream_);
+                set_mode_kernel<<<1, 1, 0, stream_>>>(st_, p, MODE_FP64);
+                PDFP_CK(cudaGetLastError());
+                vec_mode_[p] = MODE_FP64;
+                with64 = true;
+                polished_.insert(p);
+            }
+        }
+        const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+        if (wall > max_time + 120.0) throw Error(E_TIMEOUT, "solve exceeded its time limit by 120 s on the host clock");
+    }
+    std::vector<InstState> hs(K_);
+    PDFP_CK(cudaMemcpyAsync(hs.data(), st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost, stream_));
+    PDFP_CK(cudaStreamSynchronize(stream_));
+    for (int p = 0; p < K_; ++p) {
+        const InstState& s = hs[p];
+        pdfp_result& r = results[p];
+        std::memset(&r, 0, sizeof(r));
+        r.status = s.status;
+        r.restarts = s.restarts;
+        r.total_count = s.total;
+        r.rel_primal = s.rel_p;
+        r.rel_dual = s.rel_d;
+        r.rel_gap = s.rel_gap;
+        r.primal_weight = s.primal_weight;
+        r.step_size = s.step_size;
+        r.max_singular_value = s.max_sv;
+        r.fixed_point_error = s.fpe;
+        r.objective_value = s.l1;
+        r.polished = polished_.count(p) ? 1 : 0;
+        r.precision = vec_mode_[p] == MODE_FP32 ? PDFP_MIXED : PDFP_FP64;
+        vec_mode_[p] = s.mode;
+    }
+    polished_.clear();
+}
+
+void Projector::profile_step(int iterations, float* ms_primal, float* ms_dual, double* bytes_primal,
+                             double* bytes_dual) {
+    // Times the two fused step kernels (minor steps) over `iterations` steps of
+    // every running instance, with events around each launch on the stream.
+    const bool mixed = precision_ == PDFP_MIXED;
+    window_graph(200, mixed, !mixed);  // sets grid sizes and smem attributes
+    DeviceArena tmp;
+    int32_t* saved = tmp.alloc<int32_t>(K_);
+    swap_status_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, saved, K_, 0);
+    PDFP_CK(cudaGetLastError());
+    cudaEvent_t e[3];
+    for (auto& x : e) PDFP_CK(cudaEventCreate(&x));
+    float tp = 0.f, td = 0.f;
+    for (int i = 0; i < iterations; ++i) {
+        const int k = 2 + (i % 150);
+        PDFP_CK(cudaEventRecord(e[0], stream_));
+        if (mixed) launch_tile(it_t_.dev, PrimalOp<float, false, NT_ITER>{v32_, st_, k, MODE_FP32, err_}, g_.p32, stream_);
+        else launch_tile(it_t_.dev, PrimalOp<double, false, NT_ITER>{v64_, st_, k, MODE_FP64, err_}, g_.p64, stream_);
+        PDFP_CK(cudaEventRecord(e[1], stream_));
+        if (mixed) launch_tile(it_a_.dev, DualOp<float, false, NT_ITER>{v32_, st_, M_.row_off, M_.n_eq, k, MODE_FP32, err_}, g_.d32, stream_);
+        else launch_tile(it_a_.dev, DualOp<double, false, NT_ITER>{v64_, st_, M_.row_off, M_.n_eq, k, MODE_FP64, err_}, g_.d64, stream_);
+        PDFP_CK(cudaEventRecord(e[2], stream_));
+        PDFP_CK(cudaEventSynchronize(e[2]));
+        float a = 0.f, b = 0.f;
+        PDFP_CK(cudaEventElapsedTime(&a, e[0], e[1]));
+        PDFP_CK(cudaEventElapsedTime(&b, e[1], e[2]));
+        tp += a;
+        td += b;
+    }
+    for (auto& x : e) cudaEventDestroy(x);
+    swap_status_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, saved, K_, 1);
+    PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaStreamSynchronize(stream_));
+    *ms_primal = iterations > 0 ? tp / iterations : 0.f;
+    *ms_dual = iterations > 0 ? td / iterations : 0.f;
+    const HostLayout& L = M_.L;
+    const double sv = mixed ? 4.0 : 8.0;
+    // algorithmic bytes: A' (values + indices + row pointers), 8 n-vectors read,
+    // 3 written, z gathered once / A, 3 m-vectors read, 1 written, x_bar gathered once
+    *bytes_primal = L.NNZ * (sv + 4.0) + 4.0 * (L.N + 1) + sv * (11.0 * L.N) + sv * L.M;
+    *bytes_dual = L.NNZ * (sv + 4.0) + 4.0 * (L.M + 1) + sv * (4.0 * L.M) + sv * L.N;
+}
+
+}  // namespace pdfp
