@@ -1,0 +1,390 @@
+"""Benchmark: PDHG iterations/s of the projector on the bandwidth-roofline workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the largest single-GPU configuration): a synthetic 1,000,000 x
+2,000,000 LP relaxation with 20,000,000 nonzeros, Zipf(1.5) row lengths capped
+at 10,000 and rescaled to exactly 20M, U[-1, 1] values, half binary columns;
+seeded synthetic data stands in for the MIPLIB instances the reference is
+measured on.  One step is one projection to a relative KKT tolerance of 1e-4
+(gap and dual residual 1e-4, primal residual 1e-5: the pump at its gap floor),
+warm-started from the previous projection with 5% of the integer targets
+flipped.  `value` = PDHG iterations of the timed projections / their device
+time (CUDA events on the library's stream), mixed precision; the plain FP64
+form is measured on the same sequence of targets and reported beside it.
+With N > 1 every rank solves its own replica (a single projection does not
+shard) and `value` sums iterations over ranks / max time.
+
+--impl reference times the reference's own CPU algorithm (the C restatement
+under oracle/, every host thread) on a bounded sample of the same workload:
+each step runs a fixed number of PDHG iterations of the same projection.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PDHG iters/s and HBM GB/s, FP32+FP64 batched vs plain FP64 at 1e-4 KKT"
+WORKLOAD = ("zipf-lp 1,000,000 x 2,000,000, 20,000,000 nnz, Zipf(1.5) rows capped at 10,000, "
+            "U[-1,1] values, 50% binary; projections warm-started with 5% of integer targets "
+            "flipped; eps_opt 1e-4, eps_feas 1e-5")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def allreduce(world, value, op="max"):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def build_workload(args, scaler="gpu"):
+    """The scaled projection problem (host arrays) and the first target.  `scaler` picks
+    scale_problem on the GPU (our arm) or in the CPU oracle (the reference arm)."""
+    from pdfp_b200 import synthetic
+    t = time.time()
+    if args.workload == "zipf-lp":
+        milp, xf = synthetic.zipf_lp(seed=1, m=args.m, n=args.n, nnz=args.nnz)
+    else:
+        milp, _, _ = synthetic.general_integer(seed=1)
+    log(f"[bench] generated {milp.A.shape} nnz={milp.A.nnz} in {time.time() - t:.1f}s")
+    n = len(milp.c)
+    con_lb = np.where(milp.is_eq, milp.b, -np.inf)
+    t = time.time()
+    if scaler == "gpu":
+        from pdfp_b200 import gpu
+        sc = gpu.scale_problem(milp.A, np.zeros(n), milp.l, milp.u, con_lb, milp.b,
+                               bound_objective_rescaling=False)
+    else:
+        from oracle import oracle as O
+        sc = O.scale_problem(milp.A, np.zeros(n), milp.l, milp.u, con_lb, milp.b,
+                             bound_objective_rescaling=False)
+    log(f"[bench] scaled ({scaler}) in {time.time() - t:.1f}s")
+    w = np.ones(n)
+    w[milp.int_idx] = sc.D_c[milp.int_idx]
+    rng = np.random.Generator(np.random.PCG64(7))
+    I = milp.int_idx
+    xt0 = np.zeros(n)
+    xt0[I] = np.round(np.clip(rng.random(len(I)) * (milp.u[I] - milp.l[I]) + milp.l[I],
+                              milp.l[I], milp.u[I]))
+    return milp, sc, w, xt0, I
+
+
+def flip_targets(xt, I, milp, rng, frac=0.05):
+    """Flip 5% of the integer targets (binary: 1 - v; general: move by one inside the bounds)."""
+    xt = xt.copy()
+    k = max(1, int(frac * len(I)))
+    idx = I[rng.choice(len(I), size=k, replace=False)]
+    up = np.minimum(xt[idx] + 1, milp.u[idx])
+    dn = np.maximum(xt[idx] - 1, milp.l[idx])
+    xt[idx] = np.where(up != xt[idx], up, dn)
+    return xt
+
+
+def run_projections(state, sc, xt_seq, params, timed):
+    """Project each target (set_target -> solve -> read x) and collect per-step figures."""
+    out = []
+    for xt in xt_seq:
+        t0 = time.perf_counter()
+        state.set_target(xt / sc.D_c)
+        state.solve(params, 1.0)
+        x = state.pdhg_x
+        t1 = time.perf_counter()
+        r = state.last
+        out.append({"iters": r["total_count"], "device_ms": r["device_ms"], "wall_s": t1 - t0,
+                    "status": r["status"], "polished": r["polished"], "rel_gap": r["rel_gap"],
+                    "kernel_ms_primal": r["kernel_ms_primal"], "kernel_ms_dual": r["kernel_ms_dual"],
+                    "kernel_samples": r["kernel_samples"], "x_sum": float(np.sum(x))})
+        if timed:
+            log(f"[bench]   {r['status']} iters={r['total_count']} device={r['device_ms']:.1f}ms "
+                f"wall={1e3 * (t1 - t0):.1f}ms polished={r['polished']}")
+    return out
+
+
+def cpu_baseline(sc, w, xt0, is_eq, is_int, threads, iterations, label):
+    """The oracle's PDHG steps on the same scaled problem: iterations/s on `threads` host threads."""
+    from oracle import oracle as O
+    O.set_threads(threads)
+    o = O.OraclePDFP(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w)
+    o.set_target(xt0 / sc.D_c)
+    step = 0.998 / np.sqrt(1.0 + 1.0)  # ||A|| <= 1 after Pock-Chambolle scaling; fixed for timing
+    o.steps(step, 1.0, 1, 2)  # warm the caches
+    t = time.perf_counter()
+    o.steps(step, 1.0, 3, iterations)
+    dt = time.perf_counter() - t
+    return {"value": iterations / dt, "unit": "iters/s", "cores": threads, "kind": "port",
+            "sample": f"{iterations} PDHG iterations of the same projection ({label}), "
+                      f"{dt:.1f}s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["zipf-lp", "general-integer"], default="zipf-lp")
+    ap.add_argument("--m", type=int, default=1_000_000)
+    ap.add_argument("--n", type=int, default=2_000_000)
+    ap.add_argument("--nnz", type=int, default=20_000_000)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-iterations", type=int, default=40)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+
+    from pdfp_b200 import gpu
+    from pdfp_b200.params import SolverParameters
+    milp, sc, w, xt0, I = build_workload(args)
+    is_eq, is_int = milp.is_eq, milp.is_int
+    params = SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-5,
+                              iteration_limit=2_000_000)
+    rng = np.random.Generator(np.random.PCG64(11 + 0 * rank))
+    seq = [xt0]
+    for _ in range(args.warmup + args.steps - 1):
+        seq.append(flip_targets(seq[-1], I, milp, rng))
+    warm, timed = seq[:args.warmup], seq[args.warmup:]
+
+    results = {}
+    for precision in (["mixed"] if args.no_fp64 else ["mixed", "fp64"]):
+        t = time.time()
+        st = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w,
+                           precision=precision)
+        tun = (gpu.C.c_int32 * 8)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning(st._h, tun))
+        tuning = {"a_t_stage_bytes": tun[0], "a_t_threads": tun[1], "a_t_tiles": tun[2],
+                  "a_stage_bytes": tun[3], "a_threads": tun[4], "a_tiles": tun[5],
+                  "a_t_gather_l2": tun[6], "a_gather_l2": tun[7]}
+        tms = (gpu.C.c_float * 64)()
+        tcfg = (gpu.C.c_int32 * 256)()
+        cnt = gpu.C.c_int32()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_table(st._h, tms, tcfg, 64, gpu.C.byref(cnt)))
+        for i in range(cnt.value):
+            log(f"[bench]   tune side={'A' if tcfg[4*i] else 'At'} stage={tcfg[4*i+1]} "
+                f"nt={tcfg[4*i+2]} l2={tcfg[4*i+3]}: {tms[i]*1e3:.1f} us")
+        log(f"[bench] {precision} handle built in {time.time() - t:.1f}s, tuning {tuning}")
+        run_projections(st, sc, warm, params, False)
+        gpu.L.check(gpu.L.lib().pdfp_set_kernel_timing(st._h, 1))
+        barrier(world)
+        with ClockSampler(local) as clk:
+            steps = run_projections(st, sc, timed, params, True)
+        barrier(world)
+        iters = sum(s["iters"] for s in steps)
+        dev_s = sum(s["device_ms"] for s in steps) / 1e3
+        wall_s = sum(s["wall_s"] for s in steps)
+        max_dev = allreduce(world, dev_s, "max")
+        max_wall = allreduce(world, wall_s, "max")
+        tot_iters = allreduce(world, iters, "sum")
+        kp = [s["kernel_ms_primal"] for s in steps if s["kernel_samples"]]
+        kd = [s["kernel_ms_dual"] for s in steps if s["kernel_samples"]]
+        results[precision] = {"tuning": tuning, "iters": iters, "tot_iters": tot_iters, "dev_s": max_dev,
+                              "wall_s": max_wall, "steps": steps, "clocks": clk.summary(),
+                              "kp_ms": float(np.mean(kp)) if kp else None,
+                              "kd_ms": float(np.mean(kd)) if kd else None}
+        del st
+
+    if rank != 0:
+        barrier(world)
+        return
+    mx = results["mixed"]
+    A = sc.A
+    nnz, n, m = A.nnz, A.shape[1], A.shape[0]
+    # algorithmic bytes per PDHG iteration (FP32): both sides read A once (4 B value + 4 B index),
+    # row pointers once, every vector once (n-side 8 reads + 3 writes, m-side 3 + 1), and the
+    # two gathered vectors once
+    bytes_iter32 = 16.0 * nnz + 4.0 * (n + 1) + 4.0 * (m + 1) + 4.0 * 11 * n + 4.0 * 4 * m + 4.0 * (n + m)
+    bytes_primal32 = 8.0 * nnz + 4.0 * (n + 1) + 4.0 * 11 * n + 4.0 * m
+    value = mx["tot_iters"] / mx["dev_s"]
+    peak, peak_kind = measured_hbm_peak()
+    roof = None
+    if mx["kp_ms"]:
+        achieved = bytes_primal32 / (mx["kp_ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "kernel": f"tile_spmv_kernel<PrimalOp<float, false, {mx['tuning']['a_t_threads']}>> (A'z + fused primal/y update)",
+                "peak_kind": peak_kind, "bytes_per_launch": bytes_primal32,
+                "mean_launch_ms": round(mx["kp_ms"], 5),
+                "dual_kernel_mean_launch_ms": round(mx["kd_ms"], 5) if mx["kd_ms"] else None}
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * mx["dev_s"] / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD if args.workload == "zipf-lp" else "general-integer 20k x 50k",
+                   "m": m, "n": n, "nnz": nnz, "precision": "mixed (FP32 iterates and SpMV, FP64 "
+                   "reductions, restart logic and polish)", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (~450 MB streamed per iteration)",
+                   "tuning": mx["tuning"]},
+        "hbm_gbs": round(bytes_iter32 * value / world / 1e9, 1),
+        "iterations_per_step": [s["iters"] for s in mx["steps"]],
+        "status_per_step": [s["status"] for s in mx["steps"]],
+    }
+    if "fp64" in results:
+        fp = results["fp64"]
+        fv = fp["tot_iters"] / fp["dev_s"]
+        line["fp64_plain"] = {"value": round(fv, 1), "unit": "iters/s",
+                              "ms_per_step": round(1e3 * fp["dev_s"] / args.steps, 3),
+                              "iterations_per_step": [s["iters"] for s in fp["steps"]],
+                              "kernel_primal_ms": fp["kp_ms"]}
+        line["speedup_vs_fp64_plain"] = round(value / fv, 3)
+        line["time_speedup_vs_fp64_plain"] = round(fp["dev_s"] / mx["dev_s"], 3)
+    line["roofline"] = roof
+    h2d = 8 * n * args.steps
+    line["e2e"] = {"value": round(mx["tot_iters"] / mx["wall_s"], 1), "unit": "iters/s",
+                   "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                   "note": "set_target (host -> device) + solve + pdhg_x (device -> host) per step, "
+                           "host wall clock"}
+    windows = mx["iters"] // 200
+    line["gpu_launches"] = int(windows * (2 * 200 + 10) + args.steps * 12)
+    line["clocks"] = mx["clocks"]
+    if not args.no_cpu_baseline:
+        t = time.time()
+        line["cpu_baseline"] = cpu_baseline(sc, w, xt0, is_eq, is_int, 1, args.cpu_iterations,
+                                            "single thread")
+        log(f"[bench] cpu baseline in {time.time() - t:.1f}s")
+    else:
+        line["cpu_baseline"] = None
+    print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    milp, sc, w, xt0, I = build_workload(args, scaler="oracle")
+    threads = os.cpu_count() or 1
+    per_step = max(1, args.cpu_iterations // 4)
+    from oracle import oracle as O
+    O.set_threads(threads)
+    o = O.OraclePDFP(sc.A, sc.con_ub, milp.is_eq, milp.is_int, sc.var_lb, sc.var_ub, w)
+    o.set_target(xt0 / sc.D_c)
+    step = 0.998 / np.sqrt(2.0)
+    for k in range(args.warmup):
+        o.steps(step, 1.0, 1 + k * per_step, per_step)
+    t = time.perf_counter()
+    for k in range(args.steps):
+        o.steps(step, 1.0, 1 + (args.warmup + k) * per_step, per_step)
+    dt = time.perf_counter() - t
+    value = args.steps * per_step / dt
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "iters/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * dt / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp64 (the reference's CPU path)"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "iters/s", "cores": threads,
+                             "kind": "port", "sample": f"{per_step} PDHG iterations per step of "
+                             "the same projection on the C restatement of the reference's CPU "
+                             f"path, {threads} threads"},
+            "e2e": {"value": round(value, 3), "unit": "iters/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

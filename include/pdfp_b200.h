@@ -102,8 +102,12 @@ typedef struct {
     double rel_primal, rel_dual, rel_gap;
     double primal_weight, step_size, max_singular_value, fixed_point_error;
     double objective_value;      /* PDLP: c'x in original units; PDFP: l1 distance sum_I w|x - x~| (scaled data) */
-    int32_t polished;            /* MIXED: iterations finished in the FP64 polish */
-    int32_t precision;           /* arithmetic at termination */
+    int32_t polished;            /* MIXED: 1 if the FP64 polish finished this solve */
+    int32_t precision;           /* arithmetic at termination (PDFP_FP64 / PDFP_MIXED) */
+    double device_ms;            /* device time of the solve: CUDA events on the handle's stream */
+    double kernel_ms_primal;     /* timing mode: mean device time of the A'-side step kernel */
+    double kernel_ms_dual;       /* timing mode: mean device time of the A-side step kernel */
+    int64_t kernel_samples;      /* timing mode: launches sampled per kernel */
 } pdfp_result;
 
 /* One projection problem (the data of PDFPState, src/pdfp.jl:15-52), already
@@ -171,6 +175,23 @@ PDFP_API int pdfp_get_x(pdfp_handle* h, int32_t instance, double* x_scaled);
 PDFP_API int pdfp_shape(const pdfp_handle* h, int32_t instance, int32_t* k, int32_t* m, int32_t* n);
 /* Release every device buffer of the handle (the Julia finalizer). */
 PDFP_API int pdfp_destroy(pdfp_handle* h);
+
+/* Timing mode: when on, every evaluation window of later solves also records
+ * CUDA events around two of its step launches per kernel, and pdfp_result
+ * reports their mean durations (benchmark support; off by default). */
+PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
+
+/* The step-kernel configuration the autotuner chose at creation (it times
+ * every candidate shared-memory stage size x block size on the handle's own
+ * matrix; set PDFP_AUTOTUNE=0 to use the default): out[8] = {A' stage bytes,
+ * A' threads per role, A' tiles, A stage bytes, A threads per role, A tiles,
+ * A' gathers L2-only, A gathers L2-only}. */
+PDFP_API int pdfp_get_tuning(const pdfp_handle* h, int32_t* out);
+/* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
+ * launch time, cfg[4i..4i+3] = {side (0: A', 1: A), stage bytes, threads per
+ * role, gathers L2-only}; *count receives the number of rows. */
+PDFP_API int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
+                                   int32_t* count);
 
 /* Kernel timing of the two fused PDHG step kernels, over `iterations` steps
  * of instance state as it stands (benchmark support; state advances). ms_*

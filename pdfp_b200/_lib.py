@@ -66,6 +66,10 @@ class Result(C.Structure):
         ("objective_value", C.c_double),
         ("polished", C.c_int32),
         ("precision", C.c_int32),
+        ("device_ms", C.c_double),
+        ("kernel_ms_primal", C.c_double),
+        ("kernel_ms_dual", C.c_double),
+        ("kernel_samples", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -97,6 +101,9 @@ SIGNATURES = {
     "pdfp_get_x": (C.c_int, [vp, C.c_int32, dp]),
     "pdfp_shape": (C.c_int, [vp, C.c_int32, ip, ip, ip]),
     "pdfp_destroy": (C.c_int, [vp]),
+    "pdfp_set_kernel_timing": (C.c_int, [vp, C.c_int32]),
+    "pdfp_get_tuning": (C.c_int, [vp, ip]),
+    "pdfp_get_tuning_table": (C.c_int, [vp, C.POINTER(C.c_float), ip, C.c_int32, ip]),
     "pdfp_profile_step": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                     dp, dp]),
     "pdfp_scale_problem": (C.c_int, [C.POINTER(Csr), dp, dp, dp, dp, dp, C.c_int32, C.c_double,
@@ -158,9 +165,10 @@ def uptr(a):
 def make_csr(A):
     """(Csr struct, keep-alive arrays) for a scipy sparse matrix (sorted CSR, int32)."""
     import scipy.sparse as sp
-    A = sp.csr_matrix(A, dtype=np.float64)
-    A.sum_duplicates()
-    A.sort_indices()
+    if not (sp.isspmatrix_csr(A) and A.dtype == np.float64 and A.has_canonical_format):
+        A = sp.csr_matrix(A, dtype=np.float64)
+        A.sum_duplicates()
+        A.sort_indices()
     rp = np.ascontiguousarray(A.indptr, dtype=np.int32)
     ci = np.ascontiguousarray(A.indices, dtype=np.int32)
     v = np.ascontiguousarray(A.data, dtype=np.float64)

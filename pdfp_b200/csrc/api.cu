@@ -197,6 +197,28 @@ int pdfp_destroy(pdfp_handle* h) {
     return guarded([&] { delete h; });
 }
 
+int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on) {
+    return guarded([&] {
+        if (!h) throw pdfp::Error(PDFP_E_INVALID, "null handle");
+        h->proj->set_kernel_timing(on != 0);
+    });
+}
+
+int pdfp_get_tuning(const pdfp_handle* h, int32_t* out) {
+    return guarded([&] {
+        if (!h || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->tuning(out);
+    });
+}
+
+int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
+                          int32_t* count) {
+    return guarded([&] {
+        if (!h || !count || (cap > 0 && (!ms || !cfg))) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        *count = h->proj->tuning_table(ms, cfg, cap);
+    });
+}
+
 int pdfp_profile_step(pdfp_handle* h, int32_t iterations, float* ms_primal, float* ms_dual,
                       double* bytes_primal, double* bytes_dual) {
     return guarded([&] {

@@ -10,8 +10,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#ifndef PDFP_WAIT_LIMIT
-#define PDFP_WAIT_LIMIT (1u << 24)  // try_wait polls before a wait is declared hung
+#ifndef PDFP_WAIT_LIMIT_NS
+#define PDFP_WAIT_LIMIT_NS 4000000000ull  // a device wait longer than 4 s is declared hung
 #endif
 
 namespace pdfp {
@@ -83,13 +83,70 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// try_wait with a suspend-time hint: a waiting thread sleeps (up to `ns`)
+// instead of spinning.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+// Non-blocking test of a phase (acquire on success).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// Named barrier among the first `nthreads` threads of the block (id 1..15).
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Bounded wait on an mbarrier phase.  Returns false (and records the timeout
-// in *err) if the phase did not complete within PDFP_WAIT_LIMIT polls.
+// in *err) if the phase did not complete within PDFP_WAIT_LIMIT_NS.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err) {
-    for (uint32_t i = 0; i < PDFP_WAIT_LIMIT; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    if (err) atomicExch(err, DEV_ERR_TIMEOUT);
-    return false;
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait_sleep(bar, parity, 20000u)) {
+        if (globaltimer_ns() - t0 > PDFP_WAIT_LIMIT_NS) {
+            if (err) atomicExch(err, DEV_ERR_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+
+// A group of `nthreads` threads (named barrier `id`) waits for a phase: one
+// elected thread sleeps on the barrier, the group meets at the named barrier,
+// then every thread takes its own acquire with a non-blocking test (already
+// complete, so it passes at once).  Returns false if the wait gave up.
+__device__ __forceinline__ bool group_wait(uint64_t* bar, uint32_t parity, int32_t* err,
+                                           bool elected, int id, int nthreads, int32_t* flag) {
+    if (elected && !mbar_wait_bounded(bar, parity, err)) *flag = 1;
+    named_sync(id, nthreads);
+    if (*flag) return false;
+    if (!mbar_test_wait(bar, parity)) return mbar_wait_bounded(bar, parity, err);
+    return true;
 }
 
 // Streaming loads that should not displace the gathered vectors from L2.
@@ -97,18 +154,21 @@ __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
 
 // ---- block reductions (fixed order: deterministic for a fixed block size) ----
-template <int NT, int K>
-__device__ __forceinline__ void block_sum(double (&v)[K], double* scratch /* K*NT/32 */) {
+// Sum over the first NT threads; BAR = 0 uses __syncthreads, otherwise the
+// named barrier BAR among those NT threads.
+template <int NT, int K, int BAR = 0>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* scratch /* K*NT/32 */,
+                                          int tid /* index within the NT threads */) {
 #pragma unroll
     for (int k = 0; k < K; ++k)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
     if (lane == 0)
 #pragma unroll
         for (int k = 0; k < K; ++k) scratch[k * NW + warp] = v[k];
-    __syncthreads();
+    if (BAR) named_sync(BAR, NT); else __syncthreads();
     if (warp == 0) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -118,7 +178,7 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* scratch /* K*N
             v[k] = t;
         }
     }
-    __syncthreads();
+    if (BAR) named_sync(BAR, NT); else __syncthreads();
 }
 
 }  // namespace pdfp

@@ -62,10 +62,14 @@ DeviceMatrix::Tiling DeviceMatrix::make_tiling(DeviceArena& ar, bool transpose,
     s.tile_row = ar.upload(t.host.tile_row);
     s.tile_chunk = ar.upload(t.host.tile_chunk);
     s.tile_inst = ar.upload(t.host.tile_inst);
-    s.chunk_k0 = ar.upload(t.host.chunk_k0);
-    s.chunk_k1 = ar.upload(t.host.chunk_k1);
-    s.chunk_tile = ar.upload(t.host.chunk_tile);
-    s.chunk_flags = ar.upload(t.host.chunk_flags);
+    std::vector<ChunkDesc> desc(t.host.chunk_k0.size());
+    for (size_t c = 0; c < desc.size(); ++c) {
+        const int32_t tile = t.host.chunk_tile[c];
+        desc[c] = ChunkDesc{t.host.chunk_k0[c], t.host.chunk_k1[c], t.host.tile_row[tile],
+                            t.host.tile_row[tile + 1], tile, t.host.tile_inst[tile],
+                            t.host.chunk_flags[c], t.host.tile_chunk[tile] == (int32_t)c ? 1 : 0};
+    }
+    s.chunks = ar.upload(desc);
     t.inst_tile0 = ar.upload(t.host.inst_tile0);
     return t;
 }

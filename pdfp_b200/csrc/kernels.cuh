@@ -12,18 +12,12 @@
 
 namespace pdfp {
 
-__device__ __forceinline__ uint64_t globaltimer_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
 // ---- launching the tile engine ----------------------------------------------------
 
 template <class Op>
 size_t tile_dyn_smem(const SideDev& s) {
     size_t nv = Op::NV > 0 ? Op::NV : 1;
-    return 2 * static_cast<size_t>(s.stage_bytes) +
+    return kStages * static_cast<size_t>(s.stage_bytes) +
            ((nv * s.max_tile_rows * sizeof(typename Op::AT) + 127) & ~size_t(127));
 }
 
@@ -31,10 +25,16 @@ size_t tile_dyn_smem(const SideDev& s) {
 template <class Op>
 int tile_grid(const SideDev& s, int num_sms) {
     const size_t smem = tile_dyn_smem<Op>(s);
-    cudaFuncSetAttribute(tile_spmv_kernel<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(smem));
+    // The attribute belongs to the kernel, shared by every tiling launched with
+    // it: only ever raise it.
+    static size_t attr = 0;
+    if (smem > attr) {
+        cudaFuncSetAttribute(tile_spmv_kernel<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+        attr = smem;
+    }
     int blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_spmv_kernel<Op>, Op::NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_spmv_kernel<Op>, 2 * Op::NT + 32, smem);
     const int per_sm = blocks > 0 ? blocks : 1;
     int g = per_sm * num_sms;
     return g < s.n_tiles ? g : s.n_tiles;
@@ -43,7 +43,7 @@ int tile_grid(const SideDev& s, int num_sms) {
 template <class Op>
 void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream) {
     if (s.n_tiles <= 0 || grid <= 0) return;
-    tile_spmv_kernel<Op><<<grid, Op::NT, tile_dyn_smem<Op>(s), stream>>>(s, op);
+    tile_spmv_kernel<Op><<<grid, 2 * Op::NT + 32, tile_dyn_smem<Op>(s), stream>>>(s, op);
 }
 
 // ---- per-tile elementwise reductions and per-instance finalisation ---------------
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256) tile_rows_kernel(const SideDev s, const R
     for (int k = 0; k < (NP > 0 ? NP : 1); ++k) acc[k] = 0.0;
     for (int32_t r = r0 + threadIdx.x; r < r1; r += 256) op.row(r, inst, acc);
     if (NP > 0) {
-        block_sum<256, (NP > 0 ? NP : 1)>(acc, red);
+        block_sum<256, (NP > 0 ? NP : 1)>(acc, red, threadIdx.x);
         if (threadIdx.x == 0) op.write_partials(t, acc);
     }
 }
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(const FinOp op) {
         for (int32_t t = op.tb0[p] + threadIdx.x; t < op.tb0[p + 1]; t += 256)
 #pragma unroll
             for (int k = 0; k < (NB > 0 ? NB : 1); ++k) a[NA + k] += op.pb[t * (NB > 0 ? NB : 1) + k];
-    block_sum<256, N>(a, red);
+    block_sum<256, N>(a, red, threadIdx.x);
     if (threadIdx.x == 0) op.finalize(p, a);
 }
 

@@ -70,6 +70,13 @@ PDFP_HD inline StageLayout stage_layout(int esize_v, int esize_vec, int esize_ac
     return s;
 }
 
+// Everything a kernel needs to know about one chunk, in one 32-byte load.
+struct alignas(32) ChunkDesc {
+    int32_t k0, k1;  // nonzero range of the chunk
+    int32_t r0, r1;  // rows of its tile
+    int32_t tile, inst, flags, first;  // first: this is the tile's first chunk
+};
+
 // Device view of one side of the matrix plus one tiling of it.
 struct SideDev {
     int32_t rows;
@@ -79,10 +86,7 @@ struct SideDev {
     const int32_t* tile_row;     // n_tiles + 1
     const int32_t* tile_chunk;   // n_tiles + 1: first chunk of each tile
     const int32_t* tile_inst;    // n_tiles
-    const int32_t* chunk_k0;     // n_chunks
-    const int32_t* chunk_k1;
-    const int32_t* chunk_tile;
-    const int32_t* chunk_flags;
+    const ChunkDesc* chunks;     // n_chunks
 };
 
 // Sizes of what one chunk stages (must match chunk_view in tile_spmv.cuh).

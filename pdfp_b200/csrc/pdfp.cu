@@ -11,7 +11,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <map>
 #include <memory>
 
@@ -24,7 +26,6 @@
 
 namespace pdfp {
 
-constexpr int NT_ITER = 512;
 constexpr int NT_EVAL = 256;
 constexpr int STALL_EVALS = 10;  // evaluations without 10% KKT progress before the FP64 polish
 
@@ -383,18 +384,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     K_ = L.K;
     M_.upload(ar_, precision_ == PDFP_MIXED);
 
-    // tilings
-    StageGeom git{precision_ == PDFP_MIXED ? 4 : 8, precision_ == PDFP_MIXED ? 4 : 8,
-                  precision_ == PDFP_MIXED ? 4 : 8, 8, 1, 40 * 1024, 2048};
-    it_t_ = M_.make_tiling(ar_, true, git);
-    git.nvec = 3;
-    it_a_ = M_.make_tiling(ar_, false, git);
-    if (precision_ == PDFP_MIXED) {  // FP64 tilings for the polish
-        StageGeom g64{8, 8, 8, 8, 1, 40 * 1024, 2048};
-        it64_t_ = M_.make_tiling(ar_, true, g64);
-        g64.nvec = 3;
-        it64_a_ = M_.make_tiling(ar_, false, g64);
-    }
+    // tilings of the evaluation passes (the step kernels' tilings are tuned below)
     StageGeom gev{8, 8, 8, 0, 2, 32 * 1024, 2048};
     ev_t_ = M_.make_tiling(ar_, true, gev);
     ev_a_ = M_.make_tiling(ar_, false, gev);
@@ -497,10 +487,177 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     ed_.val_a = M_.v64_a;
     ed_.part_col = part_col_;
     ed_.part_row = part_row_;
+    for (auto& e : tev_) PDFP_CK(cudaEventCreate(&e));
+    for (auto& e : sev_) PDFP_CK(cudaEventCreate(&e));
     PDFP_CK(cudaDeviceSynchronize());
+    const char* at = std::getenv("PDFP_AUTOTUNE");
+    const bool tune = !(at && at[0] == '0');
+    if (precision_ == PDFP_MIXED) {
+        if (tune) autotune(true); else { prepare_side(p32_, true, true); prepare_side(d32_, false, true); }
+    }
+    if (tune && precision_ == PDFP_FP64) {
+        autotune(false);
+    } else {
+        prepare_side(p64_, true, false);
+        prepare_side(d64_, false, false);
+    }
+}
+
+template <>
+IterVecs<float>& Projector::vecs<float>() { return v32_; }
+template <>
+IterVecs<double>& Projector::vecs<double>() { return v64_; }
+
+template <typename T, bool MAJOR>
+void Projector::launch_primal(const StepSide& s, int k) {
+    const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    if (s.nt == 256)
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_);
+    else
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_);
+}
+
+template <typename T, bool MAJOR>
+void Projector::launch_dual(const StepSide& s, int k) {
+    const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    if (s.nt == 256)
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_);
+    else
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_);
+}
+
+// Grid of a step Op family for a tiling (sets the shared-memory attribute of
+// both the MAJOR and the minor kernel).
+template <template <typename, bool, int> class OpT, typename T>
+static int step_grid(const SideDev& d, int nt, int sms) {
+    if (nt == 256) {
+        tile_grid<OpT<T, false, 256>>(d, sms);
+        return tile_grid<OpT<T, true, 256>>(d, sms);
+    }
+    tile_grid<OpT<T, false, 128>>(d, sms);
+    return tile_grid<OpT<T, true, 128>>(d, sms);
+}
+
+void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
+    const int e = f32 ? 4 : 8;
+    StageGeom g{e, e, e, primal ? 8 : 3, 1, s.stage_bytes, 2048};
+    s.tiling = M_.make_tiling(ar_, primal, g);
+    if (primal)
+        s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_)
+                     : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_);
+    else
+        s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_)
+                     : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_);
+}
+
+// The autotuner: times the minor step kernel of each side for every candidate
+// (shared-memory stage size x threads per role x gather cache policy) on this
+// handle's matrix, twice, and keeps the fastest.  Runs at creation on the
+// all-zero state, which it resets afterwards.
+void Projector::autotune(bool f32) {
+    struct Cand {
+        int stage, nt, l2;
+    };
+    // 4 stages per block: 12-16 KB stages give 3-4 blocks per SM, 24 KB two, 32-48 KB one
+    static const Cand cands[] = {
+        {12 * 1024, 128, 0}, {16 * 1024, 128, 0}, {16 * 1024, 256, 0}, {24 * 1024, 256, 0},
+        {32 * 1024, 256, 0}, {48 * 1024, 256, 0}, {16 * 1024, 256, 1}, {24 * 1024, 256, 1},
+        {32 * 1024, 256, 1}};
+    constexpr int NC = sizeof(cands) / sizeof(cands[0]);
+    cudaEvent_t e0, e1;
+    PDFP_CK(cudaEventCreate(&e0));
+    PDFP_CK(cudaEventCreate(&e1));
+    tune_table_.clear();
+    for (int side = 0; side < 2; ++side) {
+        const bool primal = side == 0;
+        std::vector<StepSide> sides(NC);
+        std::vector<float> best_ms(NC, 1e30f);
+        bool empty_side = false;
+        for (int i = 0; i < NC; ++i) {
+            sides[i].stage_bytes = cands[i].stage;
+            sides[i].nt = cands[i].nt;
+            sides[i].gather_l2 = cands[i].l2;
+            prepare_side(sides[i], primal, f32);
+            if (sides[i].grid <= 0) empty_side = true;
+        }
+        StepSide& dst = primal ? (f32 ? p32_ : p64_) : (f32 ? d32_ : d64_);
+        if (empty_side) {  // nothing to time (no rows on this side)
+            dst = sides[2];
+            continue;
+        }
+        for (int sweep = 0; sweep < 2; ++sweep) {
+            for (int i = 0; i < NC; ++i) {
+                const StepSide& s = sides[i];
+                auto run = [&](int k) {
+                    if (primal) {
+                        if (f32) launch_primal<float, false>(s, k); else launch_primal<double, false>(s, k);
+                    } else {
+                        if (f32) launch_dual<float, false>(s, k); else launch_dual<double, false>(s, k);
+                    }
+                };
+                run(2);
+                run(3);
+                if (cudaGetLastError() != cudaSuccess) continue;  // candidate cannot launch
+                PDFP_CK(cudaEventRecord(e0, stream_));
+                const int reps = 8;
+                for (int r = 0; r < reps; ++r) run(4 + r);
+                PDFP_CK(cudaEventRecord(e1, stream_));
+                PDFP_CK(cudaEventSynchronize(e1));
+                PDFP_CK(cudaGetLastError());
+                float ms = 0.f;
+                PDFP_CK(cudaEventElapsedTime(&ms, e0, e1));
+                best_ms[i] = std::min(best_ms[i], ms / reps);
+            }
+        }
+        int bi = 0;
+        for (int i = 0; i < NC; ++i) {
+            tune_table_.push_back(TuneRow{side, cands[i].stage, cands[i].nt, cands[i].l2, best_ms[i]});
+            if (best_ms[i] < best_ms[bi]) bi = i;
+        }
+        dst = sides[bi];
+        dst.tuned_ms = best_ms[bi];
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // the timing runs advanced the (all-zero) iterates: reset them
+    const HostLayout& L = M_.L;
+    const size_t es = f32 ? sizeof(float) : sizeof(double);
+    void* nvec[] = {f32 ? (void*)v32_.cx : (void*)v64_.cx, f32 ? (void*)v32_.cy : (void*)v64_.cy,
+                    f32 ? (void*)v32_.rx : (void*)v64_.rx};
+    for (void* q : nvec) PDFP_CK(cudaMemsetAsync(q, 0, es * L.N, stream_));
+    PDFP_CK(cudaMemsetAsync(f32 ? (void*)v32_.cz : (void*)v64_.cz, 0, es * L.M, stream_));
+    PDFP_CK(cudaStreamSynchronize(stream_));
+}
+
+int Projector::tuning_table(float* ms, int32_t* cfg, int cap) const {
+    const int n = static_cast<int>(tune_table_.size());
+    for (int i = 0; i < n && i < cap; ++i) {
+        ms[i] = tune_table_[i].ms;
+        cfg[4 * i + 0] = tune_table_[i].side;
+        cfg[4 * i + 1] = tune_table_[i].stage;
+        cfg[4 * i + 2] = tune_table_[i].nt;
+        cfg[4 * i + 3] = tune_table_[i].l2;
+    }
+    return n;
+}
+
+void Projector::tuning(int32_t* out) const {
+    const bool f32 = precision_ == PDFP_MIXED;
+    const StepSide& p = f32 ? p32_ : p64_;
+    const StepSide& d = f32 ? d32_ : d64_;
+    out[0] = p.stage_bytes;
+    out[1] = p.nt;
+    out[2] = p.tiling.dev.n_tiles;
+    out[3] = d.stage_bytes;
+    out[4] = d.nt;
+    out[5] = d.tiling.dev.n_tiles;
+    out[6] = p.gather_l2;
+    out[7] = d.gather_l2;
 }
 
 Projector::~Projector() {
+    for (auto& e : tev_) if (e) cudaEventDestroy(e);
+    for (auto& e : sev_) if (e) cudaEventDestroy(e);
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     graphs_.clear();
     if (flags_h_) cudaFreeHost(flags_h_);
@@ -607,30 +764,16 @@ void Projector::ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance
 void Projector::record_window(int freq, bool with32, bool with64) {
     const int mode32 = MODE_FP32, mode64 = MODE_FP64;
     auto prim32 = [&](int k, bool major) {
-        if (major)
-            launch_tile(it_t_.dev, PrimalOp<float, true, NT_ITER>{v32_, st_, k, mode32, err_}, g_.p32, stream_);
-        else
-            launch_tile(it_t_.dev, PrimalOp<float, false, NT_ITER>{v32_, st_, k, mode32, err_}, g_.p32, stream_);
+        if (major) launch_primal<float, true>(p32_, k); else launch_primal<float, false>(p32_, k);
     };
     auto dual32 = [&](int k, bool major) {
-        if (major)
-            launch_tile(it_a_.dev, DualOp<float, true, NT_ITER>{v32_, st_, M_.row_off, M_.n_eq, k, mode32, err_}, g_.d32, stream_);
-        else
-            launch_tile(it_a_.dev, DualOp<float, false, NT_ITER>{v32_, st_, M_.row_off, M_.n_eq, k, mode32, err_}, g_.d32, stream_);
+        if (major) launch_dual<float, true>(d32_, k); else launch_dual<float, false>(d32_, k);
     };
-    const DeviceMatrix::Tiling& t64 = precision_ == PDFP_MIXED ? it64_t_ : it_t_;
-    const DeviceMatrix::Tiling& a64 = precision_ == PDFP_MIXED ? it64_a_ : it_a_;
     auto prim64 = [&](int k, bool major) {
-        if (major)
-            launch_tile(t64.dev, PrimalOp<double, true, NT_ITER>{v64_, st_, k, mode64, err_}, g_.p64, stream_);
-        else
-            launch_tile(t64.dev, PrimalOp<double, false, NT_ITER>{v64_, st_, k, mode64, err_}, g_.p64, stream_);
+        if (major) launch_primal<double, true>(p64_, k); else launch_primal<double, false>(p64_, k);
     };
     auto dual64 = [&](int k, bool major) {
-        if (major)
-            launch_tile(a64.dev, DualOp<double, true, NT_ITER>{v64_, st_, M_.row_off, M_.n_eq, k, mode64, err_}, g_.d64, stream_);
-        else
-            launch_tile(a64.dev, DualOp<double, false, NT_ITER>{v64_, st_, M_.row_off, M_.n_eq, k, mode64, err_}, g_.d64, stream_);
+        if (major) launch_dual<double, true>(d64_, k); else launch_dual<double, false>(d64_, k);
     };
     auto evals = [&](int which) {
         if (with32) {
@@ -642,8 +785,18 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             launch_tile(ev_a_.dev, EvalRowOp<double, NT_EVAL>{v64_, ed_, st_, M_.row_off, M_.n_eq, which, mode64, err_}, g_.er, stream_);
         }
     };
+    const bool sample = timing_ && freq >= 3 && (with32 != with64);
     for (int i = 1; i <= freq; ++i) {
         const bool major = (i == 1 || i == freq);
+        if (sample && i == 2) {
+            // events around one minor step of each kernel (timing mode)
+            PDFP_CK(cudaEventRecordWithFlags(tev_[0], stream_, cudaEventRecordExternal));
+            if (with32) prim32(i, major); else prim64(i, major);
+            PDFP_CK(cudaEventRecordWithFlags(tev_[1], stream_, cudaEventRecordExternal));
+            if (with32) dual32(i, major); else dual64(i, major);
+            PDFP_CK(cudaEventRecordWithFlags(tev_[2], stream_, cudaEventRecordExternal));
+            continue;
+        }
         if (with32) { prim32(i, major); dual32(i, major); }
         if (with64) { prim64(i, major); dual64(i, major); }
         if (i == 1) {
@@ -659,23 +812,11 @@ void Projector::record_window(int freq, bool with32, bool with64) {
 }
 
 cudaGraphExec_t Projector::window_graph(int freq, bool with32, bool with64) {
-    const int key = freq * 4 + (with32 ? 1 : 0) + (with64 ? 2 : 0);
+    const int key = freq * 8 + (with32 ? 1 : 0) + (with64 ? 2 : 0) + (timing_ ? 4 : 0);
     auto it = graphs_.find(key);
     if (it != graphs_.end()) return it->second;
-    // persistent grid sizes (outside capture)
-    g_.p32 = precision_ == PDFP_MIXED ? tile_grid<PrimalOp<float, true, NT_ITER>>(it_t_.dev, num_sms_) : 0;
-    g_.d32 = precision_ == PDFP_MIXED ? tile_grid<DualOp<float, true, NT_ITER>>(it_a_.dev, num_sms_) : 0;
-    {
-        const DeviceMatrix::Tiling& t64 = precision_ == PDFP_MIXED ? it64_t_ : it_t_;
-        const DeviceMatrix::Tiling& a64 = precision_ == PDFP_MIXED ? it64_a_ : it_a_;
-        g_.p64 = tile_grid<PrimalOp<double, true, NT_ITER>>(t64.dev, num_sms_);
-        g_.d64 = tile_grid<DualOp<double, true, NT_ITER>>(a64.dev, num_sms_);
-        tile_grid<PrimalOp<double, false, NT_ITER>>(t64.dev, num_sms_);
-        tile_grid<DualOp<double, false, NT_ITER>>(a64.dev, num_sms_);
-    }
+    // persistent grid sizes and shared-memory attributes (outside capture)
     if (precision_ == PDFP_MIXED) {
-        tile_grid<PrimalOp<float, false, NT_ITER>>(it_t_.dev, num_sms_);
-        tile_grid<DualOp<float, false, NT_ITER>>(it_a_.dev, num_sms_);
         tile_grid<EvalColOp<float, NT_EVAL>>(ev_t_.dev, num_sms_);
         tile_grid<EvalRowOp<float, NT_EVAL>>(ev_a_.dev, num_sms_);
     }
@@ -730,6 +871,7 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         sv_tol = q.sv_tolerance;
         max_time = std::max(max_time, q.time_limit);
     }
+    PDFP_CK(cudaEventRecord(sev_[0], stream_));
     solve_begin_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, K_);
     PDFP_CK(cudaGetLastError());
     ensure_step_sizes(sv_it, sv_tol);
@@ -756,6 +898,8 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
     PDFP_CK(cudaStreamSynchronize(stream_));
     int32_t dev_err = 0;
+    double kp_sum = 0.0, kd_sum = 0.0;
+    int64_t k_samples = 0;
     for (;;) {
         bool running = false;
         for (int p = 0; p < K_; ++p) running = running || flags_h_[p].status == ST_RUNNING;
@@ -767,6 +911,14 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         PDFP_CK(cudaStreamSynchronize(stream_));
         dev_err = flags_h_[K_].status;
         if (dev_err) throw Error(E_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+        if (timing_ && freq >= 3 && (with32 != with64)) {
+            float a = 0.f, b = 0.f;
+            PDFP_CK(cudaEventElapsedTime(&a, tev_[0], tev_[1]));
+            PDFP_CK(cudaEventElapsedTime(&b, tev_[1], tev_[2]));
+            kp_sum += a;
+            kd_sum += b;
+            ++k_samples;
+        }
         // FP64 polish for instances whose FP32 progress stalled
         for (int p = 0; p < K_; ++p) {
             if (flags_h_[p].polish_request && flags_h_[p].status == ST_RUNNING && vec_mode_[p] == MODE_FP32) {
@@ -783,9 +935,12 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
         if (wall > max_time + 120.0) throw Error(E_TIMEOUT, "solve exceeded its time limit by 120 s on the host clock");
     }
+    PDFP_CK(cudaEventRecord(sev_[1], stream_));
     std::vector<InstState> hs(K_);
     PDFP_CK(cudaMemcpyAsync(hs.data(), st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost, stream_));
     PDFP_CK(cudaStreamSynchronize(stream_));
+    float solve_ms = 0.f;
+    PDFP_CK(cudaEventElapsedTime(&solve_ms, sev_[0], sev_[1]));
     for (int p = 0; p < K_; ++p) {
         const InstState& s = hs[p];
         pdfp_result& r = results[p];
@@ -802,7 +957,11 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         r.fixed_point_error = s.fpe;
         r.objective_value = s.l1;
         r.polished = polished_.count(p) ? 1 : 0;
-        r.precision = vec_mode_[p] == MODE_FP32 ? PDFP_MIXED : PDFP_FP64;
+        r.precision = s.mode == MODE_FP32 ? PDFP_MIXED : PDFP_FP64;
+        r.device_ms = solve_ms;
+        r.kernel_ms_primal = k_samples ? kp_sum / k_samples : 0.0;
+        r.kernel_ms_dual = k_samples ? kd_sum / k_samples : 0.0;
+        r.kernel_samples = k_samples;
         vec_mode_[p] = s.mode;
     }
     polished_.clear();
@@ -824,11 +983,9 @@ void Projector::profile_step(int iterations, float* ms_primal, float* ms_dual, d
     for (int i = 0; i < iterations; ++i) {
         const int k = 2 + (i % 150);
         PDFP_CK(cudaEventRecord(e[0], stream_));
-        if (mixed) launch_tile(it_t_.dev, PrimalOp<float, false, NT_ITER>{v32_, st_, k, MODE_FP32, err_}, g_.p32, stream_);
-        else launch_tile(it_t_.dev, PrimalOp<double, false, NT_ITER>{v64_, st_, k, MODE_FP64, err_}, g_.p64, stream_);
+        if (mixed) launch_primal<float, false>(p32_, k); else launch_primal<double, false>(p64_, k);
         PDFP_CK(cudaEventRecord(e[1], stream_));
-        if (mixed) launch_tile(it_a_.dev, DualOp<float, false, NT_ITER>{v32_, st_, M_.row_off, M_.n_eq, k, MODE_FP32, err_}, g_.d32, stream_);
-        else launch_tile(it_a_.dev, DualOp<double, false, NT_ITER>{v64_, st_, M_.row_off, M_.n_eq, k, MODE_FP64, err_}, g_.d64, stream_);
+        if (mixed) launch_dual<float, false>(d32_, k); else launch_dual<double, false>(d64_, k);
         PDFP_CK(cudaEventRecord(e[2], stream_));
         PDFP_CK(cudaEventSynchronize(e[2]));
         float a = 0.f, b = 0.f;

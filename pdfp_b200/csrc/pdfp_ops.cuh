@@ -75,6 +75,7 @@ struct PrimalOp {
     const InstState* st;
     int32_t k_offset, mode;
     int32_t* errp;
+    int32_t gather_l2;  // 1: gathers cached in L2 only (ld.global.cg)
 
     __device__ const T* values() const { return v.val_t; }
     __device__ const T* staged(int k) const {
@@ -94,7 +95,9 @@ struct PrimalOp {
         return st[inst].status == ST_RUNNING && st[inst].mode == mode;
     }
     __device__ TileP tile_params(int inst) const { return step_params<T>(st[inst], k_offset); }
-    __device__ void gather(int32_t col, T (&g)[1]) const { g[0] = v.cz[col]; }
+    __device__ void gather(int32_t col, T (&g)[1]) const {
+        g[0] = gather_l2 ? __ldcg(v.cz + col) : v.cz[col];
+    }
     __device__ void row(int32_t j, int32_t rr, int inst, const TileP& p, const T* const* sv,
                         const T (&s)[1], double*) const {
         const T cx = sv[0][rr], ix = sv[1][rr], cy = sv[2][rr], iy = sv[3][rr];
@@ -135,6 +138,7 @@ struct DualOp {
     const int32_t* n_eq;
     int32_t k_offset, mode;
     int32_t* errp;
+    int32_t gather_l2;
 
     __device__ const T* values() const { return v.val_a; }
     __device__ const T* staged(int k) const { return k == 0 ? v.cz : (k == 1 ? v.iz : v.b); }
@@ -148,7 +152,9 @@ struct DualOp {
         t.eq_end = row_off[inst] + n_eq[inst];
         return t;
     }
-    __device__ void gather(int32_t col, T (&g)[1]) const { g[0] = v.rx[col]; }
+    __device__ void gather(int32_t col, T (&g)[1]) const {
+        g[0] = gather_l2 ? __ldcg(v.rx + col) : v.rx[col];
+    }
     __device__ void row(int32_t i, int32_t rr, int inst, const TileP& t, const T* const* sv,
                         const T (&s)[1], double*) const {
         const T cz = sv[0][rr], iz = sv[1][rr], b = sv[2][rr];

@@ -47,8 +47,37 @@ class Projector {
     void profile_step(int iterations, float* ms_primal, float* ms_dual, double* bytes_primal,
                       double* bytes_dual);
     void set_polish(bool on) { polish_enabled_ = on ? 1 : 0; }
+    // Chosen step-kernel configurations: {stage_bytes, threads, tiles} for the
+    // A'-side and the A-side kernel of the handle's base precision.
+    void tuning(int32_t* out) const;
+    // Every autotuner measurement: ms[i] and cfg[4i..4i+3] = {side (0: A', 1: A),
+    // stage bytes, threads per role, gathers cached in L2 only}; returns the count.
+    int tuning_table(float* ms, int32_t* cfg, int cap) const;
+    void set_kernel_timing(bool on) { timing_ = on; }
 
   private:
+    // One side of the PDHG step: its tile geometry, block size and tiling.
+    struct StepSide {
+        int stage_bytes = 32 * 1024;
+        int nt = 256;
+        DeviceMatrix::Tiling tiling;
+        int grid = 0;
+        int gather_l2 = 0;
+        float tuned_ms = 0.f;
+    };
+    struct TuneRow {
+        int side, stage, nt, l2;
+        float ms;
+    };
+    std::vector<TuneRow> tune_table_;
+    template <typename T>
+    IterVecs<T>& vecs();
+    template <typename T, bool MAJOR>
+    void launch_primal(const StepSide& s, int k);
+    template <typename T, bool MAJOR>
+    void launch_dual(const StepSide& s, int k);
+    void prepare_side(StepSide& s, bool primal, bool f32);
+    void autotune(bool f32);
     void check_instance(int p) const;
     void ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance);
     void record_window(int freq, bool with32, bool with64);
@@ -60,7 +89,8 @@ class Projector {
     cudaStream_t stream_ = nullptr;
     DeviceArena ar_;
     DeviceMatrix M_;
-    DeviceMatrix::Tiling it_t_, it_a_, it64_t_, it64_a_, ev_t_, ev_a_;
+    DeviceMatrix::Tiling ev_t_, ev_a_;
+    StepSide p32_, d32_, p64_, d64_;
     IterVecs<double> v64_{};
     IterVecs<float> v32_{};
     EvalData ed_{};
@@ -77,9 +107,12 @@ class Projector {
     std::set<int> polished_;
     int32_t polish_enabled_ = 1;
     struct Grids {
-        int p32 = 0, d32 = 0, p64 = 0, d64 = 0, ec = 0, er = 0;
+        int ec = 0, er = 0;
     } g_;
     std::map<int, cudaGraphExec_t> graphs_;
+    bool timing_ = false;
+    cudaEvent_t tev_[3] = {nullptr, nullptr, nullptr};     // sampled step kernels (timing mode)
+    cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
 };
 
 }  // namespace pdfp

@@ -5,20 +5,29 @@
 // cut into TILES of whole rows whose data fit one shared-memory stage; a row
 // too long for a stage gets a tile of its own, split into several CHUNKS.
 //
-// A persistent kernel walks the tiles assigned to its block (round robin),
-// double buffered: while chunk u is being processed, one thread has already
-// issued the cp.async.bulk copies of chunk u+1 (row pointers, column indices,
-// values and -- on a tile's last chunk -- the slices of the per-row vectors the
-// epilogue reads) into the other stage, completing on an mbarrier.  Per chunk:
+// A persistent, warp-specialised kernel walks the tiles assigned to its block
+// (round robin) with three roles and kStages shared-memory stages:
 //
-//   1. products   p_k = a_k * g[col_k]   for every nonzero, thread-strided, so
-//                 all gathers of the chunk are in flight at once (the gathered
-//                 vector is L2-resident);
-//   2. row sums   in shared memory: G lanes per row (G = 1 sums a row
-//                 sequentially in ascending storage order, which is the
-//                 reference's order); long rows use a block reduction;
-//   3. epilogue   one thread per row, consecutive rows on consecutive threads:
-//                 the fused PDHG update (or an evaluation term) of the Op.
+//   PRODUCER  (one lane of the last warp) issues, for each chunk, the
+//             cp.async.bulk copies of the row pointers, column indices, values
+//             and -- on a tile's last chunk -- the slices of the per-row vectors
+//             the epilogue reads, completing on the stage's FULL mbarrier; it
+//             waits on the stage's EMPTY mbarrier before reusing it.
+//   GATHERERS (NT threads) wait on FULL and compute the products
+//             p_k = a_k * g[col_k] of every nonzero, thread-strided with eight
+//             gathers in flight per thread (the gathered vector is L2-resident),
+//             in place over the staged values; then arrive on PROD.
+//   REDUCERS  (NT threads) wait on PROD, sum each row in shared memory (G lanes
+//             per row; G = 1 sums a row sequentially in ascending storage order,
+//             which is the reference's order; a long row uses a block
+//             reduction accumulated over its chunks) and, on a tile's last
+//             chunk, run the epilogue -- one thread per row, consecutive rows on
+//             consecutive threads: the fused PDHG update (or an evaluation
+//             term) of the Op; then arrive on EMPTY.
+//
+// So the gathers of one chunk are in flight while the rows of the previous one
+// are reduced and updated.  Each role synchronises internally with its own
+// named barrier; every wait is bounded.
 //
 // The Op supplies the types, the gathered vectors, the staged vectors and the
 // per-row epilogue; see pdfp_ops.cuh.  Evaluation Ops also reduce per-tile
@@ -29,78 +38,73 @@
 
 namespace pdfp {
 
+constexpr int kStages = 4;     // shared-memory stages per block
+constexpr int kGatherBar = 1;  // named barrier id of the gatherer threads
+constexpr int kReduceBar = 2;  // named barrier id of the reducer threads
+
 // Where each region of a chunk lives inside a stage buffer.
-template <int NVEC>
 struct ChunkView {
-    int32_t k0, k1, r0, r1, tile;
+    ChunkDesc d;
     bool last, single;  // single: tile is one (possibly multi-chunk) long row
     StageLayout lay;
     uint32_t sh_rp, sh_ci, sh_v, sh_vec;
 };
 
 template <int NVEC, int NV>
-__device__ __forceinline__ ChunkView<NVEC> chunk_view(const SideDev& s, int32_t c, int esize_v,
-                                                      int esize_vec, int esize_acc) {
-    ChunkView<NVEC> cv;
-    cv.k0 = s.chunk_k0[c];
-    cv.k1 = s.chunk_k1[c];
-    cv.tile = s.chunk_tile[c];
-    const int32_t f = s.chunk_flags[c];
-    cv.last = (f & CHUNK_LAST) != 0;
-    cv.single = (f & CHUNK_LONG) != 0;
-    cv.r0 = s.tile_row[cv.tile];
-    cv.r1 = s.tile_row[cv.tile + 1];
-    cv.lay = stage_layout(esize_v, esize_vec, esize_acc, NVEC, NV, cv.k0, cv.k1, cv.r0, cv.r1,
-                          cv.last, cv.single);
-    cv.sh_rp = window16_shift(cv.r0, 4);
-    cv.sh_ci = window16_shift(cv.k0, 4);
-    cv.sh_v = window16_shift(cv.k0, esize_v);
-    cv.sh_vec = window16_shift(cv.r0, esize_vec);
+__device__ __forceinline__ ChunkView chunk_view(const SideDev& s, int32_t c, int esize_v,
+                                                int esize_vec, int esize_acc) {
+    ChunkView cv;
+    cv.d = s.chunks[c];
+    cv.last = (cv.d.flags & CHUNK_LAST) != 0;
+    cv.single = (cv.d.flags & CHUNK_LONG) != 0;
+    cv.lay = stage_layout(esize_v, esize_vec, esize_acc, NVEC, NV, cv.d.k0, cv.d.k1, cv.d.r0,
+                          cv.d.r1, cv.last, cv.single);
+    cv.sh_rp = window16_shift(cv.d.r0, 4);
+    cv.sh_ci = window16_shift(cv.d.k0, 4);
+    cv.sh_v = window16_shift(cv.d.k0, esize_v);
+    cv.sh_vec = window16_shift(cv.d.r0, esize_vec);
     return cv;
 }
 
 template <class Op>
 struct TileKernelSmem {
     static constexpr int NP = Op::NP > 0 ? Op::NP : 1;
-    uint64_t bar[2];
-    int32_t stage_chunk[2];
+    uint64_t full[kStages];
+    uint64_t prod[kStages];
+    uint64_t empty[kStages];
+    int32_t stage_chunk[kStages];
     int32_t flag;
-    typename Op::AT long_acc[Op::NV];
+    typename Op::AT long_acc[Op::NV > 0 ? Op::NV : 1];
     double red[(NP > 2 ? NP : 2) * (Op::NT / 32)];
 };
 
-// Issue the bulk copies of chunk c into stage buffer `buf` (one thread).
+// Issue the bulk copies of chunk c into stage buffer `buf` (producer lane).
 template <class Op>
 __device__ __forceinline__ void issue_chunk(const SideDev& s, const Op& op, int32_t c,
                                             unsigned char* buf, uint64_t* bar) {
     using MT = typename Op::MT;
     using VT = typename Op::VT;
     using AT = typename Op::AT;
-    const ChunkView<Op::NVEC> cv =
-        chunk_view<Op::NVEC, Op::NV>(s, c, sizeof(MT), sizeof(VT), sizeof(AT));
-    const uint32_t b_rp = (cv.last && !cv.single) ? window16_bytes(cv.r0, cv.r1 + 1, 4) : 0u;
-    const uint32_t b_ci = window16_bytes(cv.k0, cv.k1, 4);
-    const uint32_t b_v = window16_bytes(cv.k0, cv.k1, sizeof(MT));
-    const uint32_t b_vec = (cv.last && Op::NVEC > 0) ? window16_bytes(cv.r0, cv.r1, sizeof(VT)) : 0u;
+    const ChunkView cv = chunk_view<Op::NVEC, Op::NV>(s, c, sizeof(MT), sizeof(VT), sizeof(AT));
+    const int32_t k0 = cv.d.k0, k1 = cv.d.k1, r0 = cv.d.r0, r1 = cv.d.r1;
+    const uint32_t b_rp = (cv.last && !cv.single) ? window16_bytes(r0, r1 + 1, 4) : 0u;
+    const uint32_t b_ci = window16_bytes(k0, k1, 4);
+    const uint32_t b_v = window16_bytes(k0, k1, sizeof(MT));
+    const uint32_t b_vec = (cv.last && Op::NVEC > 0) ? window16_bytes(r0, r1, sizeof(VT)) : 0u;
     const uint32_t bytes = b_rp + b_ci + b_v + b_vec * Op::NVEC;
-    fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
-    if (b_rp)
-        bulk_copy_g2s(buf + cv.lay.off_rp, s.rp + (cv.r0 - (int32_t)cv.sh_rp), b_rp, bar);
-    if (b_ci)
-        bulk_copy_g2s(buf + cv.lay.off_ci, s.ci + (cv.k0 - (int32_t)cv.sh_ci), b_ci, bar);
-    if (b_v)
-        bulk_copy_g2s(buf + cv.lay.off_v, op.values() + (cv.k0 - (int32_t)cv.sh_v), b_v, bar);
+    if (b_rp) bulk_copy_g2s(buf + cv.lay.off_rp, s.rp + (r0 - (int32_t)cv.sh_rp), b_rp, bar);
+    if (b_ci) bulk_copy_g2s(buf + cv.lay.off_ci, s.ci + (k0 - (int32_t)cv.sh_ci), b_ci, bar);
+    if (b_v) bulk_copy_g2s(buf + cv.lay.off_v, op.values() + (k0 - (int32_t)cv.sh_v), b_v, bar);
     if (b_vec) {
 #pragma unroll
         for (int k = 0; k < Op::NVEC; ++k)
             bulk_copy_g2s(buf + cv.lay.off_vec0 + k * cv.lay.vec_stride,
-                          op.staged(k) + (cv.r0 - (int32_t)cv.sh_vec), b_vec, bar);
+                          op.staged(k) + (r0 - (int32_t)cv.sh_vec), b_vec, bar);
     }
 }
 
 // Next chunk of this block's work list, skipping tiles of inactive instances.
-// State (tile, chunk) lives in registers of thread 0.
 struct WorkIter {
     int32_t tile, chunk, chunk_end;
 };
@@ -118,34 +122,149 @@ __device__ __forceinline__ int32_t next_chunk(const SideDev& s, const Op& op, Wo
 }
 
 template <class Op>
-__global__ void __launch_bounds__(Op::NT) tile_spmv_kernel(const SideDev s, const Op op) {
+__global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDev s, const Op op) {
     using MT = typename Op::MT;
     using VT = typename Op::VT;
     using AT = typename Op::AT;
     using GT = typename Op::GT;
     constexpr int NT = Op::NT, NV = Op::NV, NVEC = Op::NVEC, NP = Op::NP;
+    constexpr int UNROLL = 8;
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     __shared__ TileKernelSmem<Op> sh;
-    unsigned char* stage[2] = {dyn_smem, dyn_smem + s.stage_bytes};
-    AT* rowsum = reinterpret_cast<AT*>(dyn_smem + 2 * (size_t)s.stage_bytes);  // [NV][max_rows]
+    AT* rowsum = reinterpret_cast<AT*>(dyn_smem + kStages * (size_t)s.stage_bytes);  // [NV][max_rows]
 
-    WorkIter it{-1, 0, 0};
     if (threadIdx.x == 0) {
-        mbar_init(&sh.bar[0], 1);
-        mbar_init(&sh.bar[1], 1);
+        for (int i = 0; i < kStages; ++i) {
+            mbar_init(&sh.full[i], 1);
+            mbar_init(&sh.prod[i], 1);
+            mbar_init(&sh.empty[i], 1);
+        }
+        sh.flag = 0;
         fence_barrier_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int st = 0; st < 2; ++st) {
-            int32_t c = next_chunk(s, op, it);
-            sh.stage_chunk[st] = c;
-            if (c >= 0) issue_chunk(s, op, c, stage[st], &sh.bar[st]);
-        }
-    }
-    __syncthreads();
 
-    uint32_t phase[2] = {0u, 0u};
+    if (threadIdx.x >= 2 * NT) {
+        // ---- producer: one lane walks the work list and issues the copies ----
+        if (threadIdx.x == 2 * NT) {
+            WorkIter it{-1, 0, 0};
+            for (uint32_t u = 0;; ++u) {
+                const int st = u % kStages;
+                if (u >= kStages &&
+                    !mbar_wait_bounded(&sh.empty[st], ((u / kStages) - 1) & 1u, op.err())) {
+                    sh.flag = 1;  // the stage was never released: stop feeding
+                    sh.stage_chunk[st] = -1;
+                    mbar_arrive(&sh.full[st]);
+                    break;
+                }
+                const int32_t c = next_chunk(s, op, it);
+                sh.stage_chunk[st] = c;
+                if (c < 0) {
+                    mbar_arrive(&sh.full[st]);  // completes the phase: the end of the work
+                    break;
+                }
+                issue_chunk(s, op, c, dyn_smem + st * (size_t)s.stage_bytes, &sh.full[st]);
+            }
+        }
+        return;
+    }
+
+    if (threadIdx.x < NT) {
+        // ---- gatherers: products of each chunk, in place over its values ----
+        const int g = threadIdx.x;
+        for (uint32_t u = 0;; ++u) {
+            const int st = u % kStages;
+            const bool ok = group_wait(&sh.full[st], (u / kStages) & 1u, op.err(), g == 0,
+                                       kGatherBar, NT, &sh.flag);
+            const int32_t c = ok ? sh.stage_chunk[st] : -1;
+            if (c >= 0 && NV > 0) {
+                unsigned char* buf = dyn_smem + st * (size_t)s.stage_bytes;
+                const ChunkView cv = chunk_view<NVEC, NV>(s, c, sizeof(MT), sizeof(VT), sizeof(AT));
+                const int32_t K = cv.d.k1 - cv.d.k0;
+                if constexpr (sizeof(MT) == 4 && sizeof(AT) == 4 && NV == 1) {
+                    // 32-bit values: the index and value windows start 16-byte
+                    // aligned with the same shift, so each thread takes four
+                    // consecutive nonzeros with 128-bit shared loads and stores
+                    const int32_t sh0 = static_cast<int32_t>(cv.sh_ci);
+                    const int4* ci4 = reinterpret_cast<const int4*>(buf + cv.lay.off_ci);
+                    float4* v4 = reinterpret_cast<float4*>(buf + cv.lay.off_v);
+                    const int32_t quads = (sh0 + K + 3) >> 2;
+                    for (int32_t q0 = g; q0 < quads; q0 += 2 * NT) {
+                        int4 cc[2];
+                        float4 aa[2];
+                        GT gv[2][4][1];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int32_t q = q0 + h * NT;
+                            if (q < quads) {
+                                cc[h] = ci4[q];
+                                aa[h] = v4[q];
+                            }
+                        }
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int32_t q = q0 + h * NT;
+                            if (q < quads) {
+                                const int32_t e = 4 * q - sh0;  // nonzero index of the quad's first lane
+                                const int cols[4] = {cc[h].x, cc[h].y, cc[h].z, cc[h].w};
+#pragma unroll
+                                for (int j = 0; j < 4; ++j)
+                                    if (e + j >= 0 && e + j < K) op.gather(cols[j], gv[h][j]);
+                            }
+                        }
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int32_t q = q0 + h * NT;
+                            if (q < quads) {
+                                const int32_t e = 4 * q - sh0;
+                                float4 p = aa[h];
+                                if (e + 0 >= 0 && e + 0 < K) p.x = mul_rn(static_cast<float>(aa[h].x), static_cast<float>(gv[h][0][0]));
+                                if (e + 1 >= 0 && e + 1 < K) p.y = mul_rn(static_cast<float>(aa[h].y), static_cast<float>(gv[h][1][0]));
+                                if (e + 2 >= 0 && e + 2 < K) p.z = mul_rn(static_cast<float>(aa[h].z), static_cast<float>(gv[h][2][0]));
+                                if (e + 3 >= 0 && e + 3 < K) p.w = mul_rn(static_cast<float>(aa[h].w), static_cast<float>(gv[h][3][0]));
+                                v4[q] = p;
+                            }
+                        }
+                    }
+                } else {
+                    const int32_t* ci_s = reinterpret_cast<const int32_t*>(buf + cv.lay.off_ci) + cv.sh_ci;
+                    MT* v_s = reinterpret_cast<MT*>(buf + cv.lay.off_v) + cv.sh_v;
+                    AT* p1 = reinterpret_cast<AT*>(v_s);
+                    AT* p2 = reinterpret_cast<AT*>(buf + cv.lay.off_p2);
+                    for (int32_t k = g; k < K; k += UNROLL * NT) {
+                        int32_t col[UNROLL];
+                        MT a[UNROLL];
+                        GT gv[UNROLL][NV > 0 ? NV : 1];
+#pragma unroll
+                        for (int q = 0; q < UNROLL; ++q) {
+                            const int32_t kk = k + q * NT;
+                            col[q] = kk < K ? ci_s[kk] : 0;
+                            a[q] = kk < K ? v_s[kk] : MT(0);
+                        }
+#pragma unroll
+                        for (int q = 0; q < UNROLL; ++q)
+                            if (k + q * NT < K) op.gather(col[q], gv[q]);
+#pragma unroll
+                        for (int q = 0; q < UNROLL; ++q) {
+                            const int32_t kk = k + q * NT;
+                            if (kk < K) {
+                                p1[kk] = mul_rn(static_cast<AT>(a[q]), static_cast<AT>(gv[q][0]));
+                                if (NV > 1)
+                                    p2[kk] = mul_rn(static_cast<AT>(a[q]), static_cast<AT>(gv[q][NV > 1 ? NV - 1 : 0]));
+                            }
+                        }
+                    }
+                }
+                named_sync(kGatherBar, NT);
+            }
+            if (g == 0) mbar_arrive(&sh.prod[st]);  // products of this stage are in place
+            if (c < 0) break;
+        }
+        return;
+    }
+
+    // ---- reducers: row sums and the epilogue ----
+    const int r = threadIdx.x - NT;
     double acc[NP > 0 ? NP : 1];
 #pragma unroll
     for (int j = 0; j < (NP > 0 ? NP : 1); ++j) acc[j] = 0.0;
@@ -153,65 +272,35 @@ __global__ void __launch_bounds__(Op::NT) tile_spmv_kernel(const SideDev s, cons
     int32_t cur_tile = -1;
 
     for (uint32_t u = 0;; ++u) {
-        const int st = u & 1;
+        const int st = u % kStages;
+        if (!group_wait(&sh.prod[st], (u / kStages) & 1u, op.err(), r == 0, kReduceBar, NT, &sh.flag))
+            break;  // a wait gave up (error recorded)
         const int32_t c = sh.stage_chunk[st];
         if (c < 0) break;
-        const bool ok = mbar_wait_bounded(&sh.bar[st], phase[st], op.err());
-        phase[st] ^= 1u;
-        if (__syncthreads_or(!ok)) break;  // a bulk copy never completed: give up (error recorded)
 
-        unsigned char* buf = stage[st];
-        const ChunkView<NVEC> cv = chunk_view<NVEC, NV>(s, c, sizeof(MT), sizeof(VT), sizeof(AT));
-        const int32_t K = cv.k1 - cv.k0;
-        const int32_t* ci_s = reinterpret_cast<const int32_t*>(buf + cv.lay.off_ci) + cv.sh_ci;
-        MT* v_s = reinterpret_cast<MT*>(buf + cv.lay.off_v) + cv.sh_v;
-        AT* p1 = reinterpret_cast<AT*>(v_s);  // products overwrite the values in place
-        AT* p2 = reinterpret_cast<AT*>(buf + cv.lay.off_p2);
-        const int32_t inst = s.tile_inst[cv.tile];
-        if (cv.tile != cur_tile) {
-            cur_tile = cv.tile;
+        unsigned char* buf = dyn_smem + st * (size_t)s.stage_bytes;
+        const ChunkView cv = chunk_view<NVEC, NV>(s, c, sizeof(MT), sizeof(VT), sizeof(AT));
+        const int32_t K = cv.d.k1 - cv.d.k0;
+        const AT* p1 = reinterpret_cast<const AT*>(reinterpret_cast<MT*>(buf + cv.lay.off_v) + cv.sh_v);
+        const AT* p2 = reinterpret_cast<const AT*>(buf + cv.lay.off_p2);
+        const int32_t inst = cv.d.inst;
+        if (cv.d.tile != cur_tile) {
+            cur_tile = cv.d.tile;
             tp = op.tile_params(inst);
         }
 
-        // 1. products
-        if (NV > 0) {
-            for (int32_t k = threadIdx.x; k < K; k += 4 * NT) {
-                int32_t col[4];
-                MT a[4];
-                GT g[4][NV > 0 ? NV : 1];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int32_t kk = k + q * NT;
-                    col[q] = kk < K ? ci_s[kk] : 0;
-                    a[q] = kk < K ? v_s[kk] : MT(0);
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (k + q * NT < K) op.gather(col[q], g[q]);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int32_t kk = k + q * NT;
-                    if (kk < K) {
-                        p1[kk] = mul_rn(static_cast<AT>(a[q]), static_cast<AT>(g[q][0]));
-                        if (NV > 1) p2[kk] = mul_rn(static_cast<AT>(a[q]), static_cast<AT>(g[q][NV - 1]));
-                    }
-                }
-            }
-        }
-        __syncthreads();
-
-        // 2. row sums
-        const int32_t R = cv.r1 - cv.r0;
+        // row sums
+        const int32_t R = cv.d.r1 - cv.d.r0;
         if (cv.single) {
             // one long row: block reduction over this chunk, accumulated over chunks
             double part[2] = {0.0, 0.0};
-            for (int32_t k = threadIdx.x; k < K; k += NT) {
+            for (int32_t k = r; k < K; k += NT) {
                 part[0] += static_cast<double>(p1[k]);
                 if (NV > 1) part[1] += static_cast<double>(p2[k]);
             }
-            block_sum<NT, 2>(part, sh.red);
-            if (threadIdx.x == 0) {
-                const bool first = (c == s.tile_chunk[cv.tile]);
+            block_sum<NT, 2, kReduceBar>(part, sh.red, r);
+            if (r == 0) {
+                const bool first = cv.d.first != 0;
                 sh.long_acc[0] = (first ? AT(0) : sh.long_acc[0]) + static_cast<AT>(part[0]);
                 if (NV > 1) sh.long_acc[NV - 1] = (first ? AT(0) : sh.long_acc[NV - 1]) + static_cast<AT>(part[1]);
             }
@@ -220,12 +309,12 @@ __global__ void __launch_bounds__(Op::NT) tile_spmv_kernel(const SideDev s, cons
             int G = 1;
             while (G < 32 && G * 2 * R <= NT) G *= 2;
             const int groups = NT / G;
-            const int gid = threadIdx.x / G, lane = threadIdx.x & (G - 1);
+            const int gid = r / G, lane = r & (G - 1);
             for (int32_t base = 0; base < R; base += groups) {
                 const int32_t rr = base + gid;
                 AT s1 = AT(0), s2 = AT(0);
                 if (rr < R) {
-                    const int32_t e0 = rp_s[rr] - cv.k0, e1 = rp_s[rr + 1] - cv.k0;
+                    const int32_t e0 = rp_s[rr] - cv.d.k0, e1 = rp_s[rr + 1] - cv.d.k0;
                     for (int32_t k = e0 + lane; k < e1; k += G) {
                         s1 = add_rn(s1, p1[k]);
                         if (NV > 1) s2 = add_rn(s2, p2[k]);
@@ -242,14 +331,14 @@ __global__ void __launch_bounds__(Op::NT) tile_spmv_kernel(const SideDev s, cons
             }
         }
 
-        // 3. epilogue on the tile's last chunk
+        // epilogue on the tile's last chunk
         if (cv.last) {
-            __syncthreads();
+            named_sync(kReduceBar, NT);
             const VT* sv[NVEC > 0 ? NVEC : 1];
 #pragma unroll
             for (int k = 0; k < NVEC; ++k)
                 sv[k] = reinterpret_cast<const VT*>(buf + cv.lay.off_vec0 + k * cv.lay.vec_stride) + cv.sh_vec;
-            for (int32_t rr = threadIdx.x; rr < R; rr += NT) {
+            for (int32_t rr = r; rr < R; rr += NT) {
                 AT sums[NV > 0 ? NV : 1];
                 if (cv.single) {
 #pragma unroll
@@ -258,22 +347,20 @@ __global__ void __launch_bounds__(Op::NT) tile_spmv_kernel(const SideDev s, cons
 #pragma unroll
                     for (int q = 0; q < NV; ++q) sums[q] = rowsum[q * s.max_tile_rows + rr];
                 }
-                op.row(cv.r0 + rr, rr, inst, tp, sv, sums, acc);
+                op.row(cv.d.r0 + rr, rr, inst, tp, sv, sums, acc);
             }
             if constexpr (NP > 0) {
-                block_sum<NT, NP>(acc, sh.red);
-                if (threadIdx.x == 0) op.write_partials(cv.tile, acc);
+                block_sum<NT, NP, kReduceBar>(acc, sh.red, r);
+                if (r == 0) op.write_partials(cv.d.tile, acc);
 #pragma unroll
-                for (int j = 0; j < (NP > 0 ? NP : 1); ++j) acc[j] = 0.0;
+                for (int j = 0; j < NP; ++j) acc[j] = 0.0;
             }
         }
-        __syncthreads();  // stage `st` fully consumed
-        if (threadIdx.x == 0) {
-            int32_t nc = next_chunk(s, op, it);
-            sh.stage_chunk[st] = nc;
-            if (nc >= 0) issue_chunk(s, op, nc, stage[st], &sh.bar[st]);
+        named_sync(kReduceBar, NT);  // stage `st` fully consumed
+        if (r == 0) {
+            fence_proxy_async_smem();  // generic-proxy writes (products) before the next bulk copy
+            mbar_arrive(&sh.empty[st]);
         }
-        __syncthreads();
     }
 }
 

@@ -50,9 +50,11 @@ class MILP:
         self.l = np.asarray(self.l, dtype=np.float64)
         self.u = np.asarray(self.u, dtype=np.float64)
         self.int_idx = np.asarray(self.int_idx, dtype=np.int64)
-        A = sp.csr_matrix(self.A, dtype=np.float64)
-        A.sum_duplicates()
-        A.sort_indices()
+        A = self.A
+        if not (sp.isspmatrix_csr(A) and A.dtype == np.float64 and A.has_canonical_format):
+            A = sp.csr_matrix(A, dtype=np.float64)
+            A.sum_duplicates()
+            A.sort_indices()
         self.A = A
         self.row_sense = [str(s) for s in self.row_sense]
         if not self.var_names:

@@ -52,6 +52,28 @@ def covering_p0201_like(seed: int = 1, m: int = 133, n: int = 201, nnz: int = 19
                 name=f"covering_{m}x{n}_s{seed}")
 
 
+def _csr_from_keys(key: np.ndarray, vals: np.ndarray, m: int, n: int) -> sp.csr_matrix:
+    """CSR matrix from sorted unique row-major keys (row * n + col): no COO round trip."""
+    rows = key // n
+    indptr = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=m), out=indptr[1:])
+    A = sp.csr_matrix((vals, (key - rows * n).astype(np.int32), indptr), shape=(m, n))
+    A.has_sorted_indices = True
+    A.has_canonical_format = True
+    return A
+
+
+def _sorted_unique(key: np.ndarray) -> np.ndarray:
+    """Sorted distinct values (sort + adjacent difference; faster than np.unique here)."""
+    key = np.sort(key)
+    if len(key) == 0:
+        return key
+    keep = np.empty(len(key), dtype=bool)
+    keep[0] = True
+    np.not_equal(key[1:], key[:-1], out=keep[1:])
+    return key[keep]
+
+
 def _rows_with_lengths(rng, lengths: np.ndarray, n: int):
     """Row index / distinct column index arrays for the given row lengths."""
     m = len(lengths)
@@ -60,12 +82,12 @@ def _rows_with_lengths(rng, lengths: np.ndarray, n: int):
     cols = rng.integers(0, n, size=total, dtype=np.int64)
     # make columns distinct within each row: sort, drop repeats, top up with fresh draws
     key = rows * n + cols
-    key = np.unique(key)
+    key = _sorted_unique(key)
     missing = total - len(key)
     while missing > 0:
         extra_rows = rng.integers(0, m, size=missing, dtype=np.int64)
         extra_cols = rng.integers(0, n, size=missing, dtype=np.int64)
-        key = np.unique(np.concatenate([key, extra_rows * n + extra_cols]))
+        key = _sorted_unique(np.concatenate([key, extra_rows * n + extra_cols]))
         missing = total - len(key)
     return key // n, key % n
 
@@ -88,7 +110,7 @@ def general_integer(seed: int = 1, m: int = 20000, n: int = 50000, m_eq: int = 5
     while np.any(vals == 0.0):
         z = vals == 0.0
         vals[z] = np.round(rng.normal(0.0, 1.0, size=int(z.sum())), 2)
-    A = sp.csr_matrix((vals, (rows, cols)), shape=(m, n))
+    A = _csr_from_keys(rows * n + cols, vals, m, n)
     n_int = int(round(0.9 * n))
     perm = rng.permutation(n)
     int_idx = np.sort(perm[:n_int])
@@ -138,7 +160,7 @@ def zipf_lp(seed: int = 1, m: int = 1_000_000, n: int = 2_000_000, nnz: int = 20
     lengths = np.minimum(lengths, n)
     rows, cols = _rows_with_lengths(rng, lengths, n)
     vals = rng.uniform(-1.0, 1.0, size=len(rows))
-    A = sp.csr_matrix((vals, (rows, cols)), shape=(m, n))
+    A = _csr_from_keys(rows * n + cols, vals, m, n)
     n_bin = n // 2
     xf = np.concatenate([rng.integers(0, 2, size=n_bin).astype(np.float64),
                          rng.uniform(0.0, 1.0, size=n - n_bin)])
@@ -163,7 +185,7 @@ def covering_packing_batch(seed: int = 1, k: int = 64, n_min: int = 1000, n_max:
         lengths = np.minimum(lengths, n)
         rows, cols = _rows_with_lengths(rng, lengths, n)
         vals = rng.integers(1, 6, size=len(rows)).astype(np.float64)
-        A = sp.csr_matrix((vals, (rows, cols)), shape=(m, n))
+        A = _csr_from_keys(rows * n + cols, vals, m, n)
         rowsum = np.asarray(A.sum(axis=1)).ravel()
         if p < k // 2:
             milp = MILP(rng.integers(1, 101, size=n).astype(np.float64), 0.0, -A,
