@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libpdfp_b200.so")
+LIB_PATH = os.environ.get("PDFP_B200_LIB") or os.path.join(_HERE, "lib", "libpdfp_b200.so")
 
 OK = 0
 E_INVALID, E_CUDA, E_NOMEM, E_TIMEOUT, E_UNSUPPORTED, E_NODEVICE = -1, -2, -3, -4, -5, -6

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     using AT = typename Op::AT;
     using GT = typename Op::GT;
     constexpr int NT = Op::NT, NV = Op::NV, NVEC = Op::NVEC, NP = Op::NP;
-    constexpr int UNROLL = 8;
+    constexpr int UNROLL = sizeof(MT) == 4 ? 16 : 8;  // scalar path: gathers in flight per thread
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     __shared__ TileKernelSmem<Op> sh;
     AT* rowsum = reinterpret_cast<AT*>(dyn_smem + kStages * (size_t)s.stage_bytes);  // [NV][max_rows]
@@ -189,12 +189,13 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                     const int4* ci4 = reinterpret_cast<const int4*>(buf + cv.lay.off_ci);
                     float4* v4 = reinterpret_cast<float4*>(buf + cv.lay.off_v);
                     const int32_t quads = (sh0 + K + 3) >> 2;
-                    for (int32_t q0 = g; q0 < quads; q0 += 2 * NT) {
-                        int4 cc[2];
-                        float4 aa[2];
-                        GT gv[2][4][1];
+                    constexpr int QH = 4;  // quads per thread per pass: 16 gathers in flight
+                    for (int32_t q0 = g; q0 < quads; q0 += QH * NT) {
+                        int4 cc[QH];
+                        float4 aa[QH];
+                        GT gv[QH][4][1];
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
+                        for (int h = 0; h < QH; ++h) {
                             const int32_t q = q0 + h * NT;
                             if (q < quads) {
                                 cc[h] = ci4[q];
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                             }
                         }
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
+                        for (int h = 0; h < QH; ++h) {
                             const int32_t q = q0 + h * NT;
                             if (q < quads) {
                                 const int32_t e = 4 * q - sh0;  // nonzero index of the quad's first lane
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                             }
                         }
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
+                        for (int h = 0; h < QH; ++h) {
                             const int32_t q = q0 + h * NT;
                             if (q < quads) {
                                 const int32_t e = 4 * q - sh0;
