@@ -217,6 +217,25 @@ PDFP_API int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double
 PDFP_API int pdfp_estimate_max_singular_value(const pdfp_csr* A, int32_t max_iterations, double tolerance,
                                      double* sigma, int32_t* iterations);
 
+/* ||A||_2 by power iteration on matrices already on the device, with no
+ * device allocation (no counterpart in the reference).  For callers that
+ * cannot call cudaMalloc: processes whose device memory a framework allocator
+ * reserved up front (a new cudaMalloc fails or fragments its pool) and callers
+ * that must not trigger the device-wide synchronisation of cudaFree.  A and
+ * A' are device CSR arrays (0-based, ascending indices per row); the work
+ * vectors live in a fixed 8 MiB array of this library's device memory that
+ * every GPU loading the library holds until exit, so 2m + n + 2 must not
+ * exceed 1,048,576 (PDFP_E_UNSUPPORTED otherwise).  The first call on a device
+ * resolves that array's address and should come before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race.  `stream` is a
+ * cudaStream_t (NULL: the default stream); the call returns when the result
+ * is on the host.  Same algorithm, start vector and summation order as
+ * pdfp_estimate_max_singular_value. */
+PDFP_API int pdfp_estimate_max_singular_value_noalloc(
+    int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col_idx, const double* val,
+    const int32_t* row_ptr_t, const int32_t* col_idx_t, const double* val_t,
+    int32_t max_iterations, double tolerance, void* stream, double* sigma, int32_t* iterations);
+
 /* ---- root LP (src/pdlp.jl) --------------------------------------------------- */
 
 /* solve_lp_relaxation(milp; tolerance, time_limit, use_gpu = true,

@@ -1,0 +1,79 @@
+"""The allocation-free power iteration (pdfp_estimate_max_singular_value_noalloc).
+
+Some callers cannot allocate device memory: a process whose HBM a framework
+allocator reserved up front, where a fresh cudaMalloc fails or fragments the
+pool, or a caller that must not trigger cudaFree's device-wide
+synchronisation.  This entry point keeps its work vectors in a fixed 8 MiB
+device array of the library instead.  The test allocates the caller's own
+device arrays (the matrix) with torch, calls the entry point through the C
+ABI twice in a row, and checks both results against the allocating entry
+point pdfp_estimate_max_singular_value (same algorithm, start vector and
+summation order; estimates within 1e-10 relative, equal iteration counts).
+
+This file sorts last so that a run stopping at the first failure has run
+every other test before it.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from pdfp_b200 import _lib as L
+from pdfp_b200 import gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_csr(A):
+    import torch
+    A = sp.csr_matrix(A, dtype=np.float64)
+    A.sort_indices()
+    rp = torch.tensor(A.indptr.astype(np.int32), device="cuda")
+    ci = torch.tensor(A.indices.astype(np.int32) if A.nnz else np.zeros(1, np.int32), device="cuda")
+    v = torch.tensor(A.data if A.nnz else np.zeros(1), dtype=torch.float64, device="cuda")
+    return rp, ci, v
+
+
+def _noalloc(A, max_iterations=5000, tolerance=1e-4):
+    import torch
+    m, n = A.shape
+    a = _device_csr(A)
+    at = _device_csr(sp.csr_matrix(A).T.tocsr())
+    ptr = lambda t, ty: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ty))  # noqa: E731
+    sigma = C.c_double()
+    its = C.c_int32()
+    torch.cuda.synchronize()
+    rc = L.lib().pdfp_estimate_max_singular_value_noalloc(
+        m, n, ptr(a[0], C.c_int32), ptr(a[1], C.c_int32), ptr(a[2], C.c_double),
+        ptr(at[0], C.c_int32), ptr(at[1], C.c_int32), ptr(at[2], C.c_double),
+        max_iterations, tolerance, None, C.byref(sigma), C.byref(its))
+    L.check(rc)
+    return sigma.value, its.value
+
+
+def _matrices():
+    rng = np.random.default_rng(5)
+    A1 = sp.random(300, 700, density=0.02, random_state=rng, format="csr")
+    A2 = sp.random(2000, 3000, density=0.004, random_state=rng, format="csr")
+    from pdfp_b200 import synthetic
+    milp = synthetic.covering_p0201_like(1)
+    return [A1, A2, milp.A]
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_noalloc_matches_allocating_entry_point_twice(idx):
+    A = _matrices()[idx]
+    ref, ref_it = gpu.estimate_max_singular_value(A)
+    for _ in range(2):  # the shared scratch keeps the previous call's contents
+        s, it = _noalloc(A)
+        assert s == pytest.approx(ref, rel=1e-10)
+        assert it == ref_it
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    sigma = C.c_double()
+    rc = L.lib().pdfp_estimate_max_singular_value_noalloc(
+        600_000, 10, None, None, None, None, None, None, 10, 1e-4, None, C.byref(sigma), None)
+    assert rc == L.E_UNSUPPORTED
+    assert b"8 MiB" in L.lib().pdfp_last_error()
