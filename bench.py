@@ -225,7 +225,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["zipf-lp", "general-integer"], default="zipf-lp")
+    ap.add_argument("--workload", choices=["zipf-lp", "general-integer", "batch-uneven",
+                                           "pump-markshare"], default="zipf-lp")
     ap.add_argument("--m", type=int, default=1_000_000)
     ap.add_argument("--n", type=int, default=2_000_000)
     ap.add_argument("--nnz", type=int, default=20_000_000)
@@ -238,6 +239,10 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return reference_arm(args, world, rank)
+    if args.workload == "batch-uneven":
+        return batch_uneven(args, world, rank, local)
+    if args.workload == "pump-markshare":
+        return pump_markshare(args, world, rank)
 
     from pdfp_b200 import gpu
     from pdfp_b200.params import SolverParameters
@@ -352,6 +357,178 @@ def main():
         line["cpu_baseline"] = None
     print(json.dumps(line), flush=True)
     barrier(world)
+
+
+def batch_uneven(args, world, rank, local):
+    """64 uneven binary covering/packing projections packed into one batch handle.
+
+    Instances: n log-uniform in [1000, 200000], m = 0.6 n, 10-40 nonzeros per row
+    (seed 1, about 36M nonzeros in all).  One step projects a new target for every
+    instance (5% of the previous targets flipped) to eps_opt 1e-4 / eps_feas 1e-5,
+    each instance with its own restart and termination state.  value = PDHG
+    iterations summed over instances / device time of the batched solves.
+    """
+    from pdfp_b200 import gpu, synthetic
+    from pdfp_b200.params import SolverParameters
+    t = time.time()
+    models = synthetic.covering_packing_batch(seed=1 + rank)
+    log(f"[bench] generated {len(models)} models, nnz={sum(mm.A.nnz for mm in models)} "
+        f"in {time.time() - t:.1f}s")
+    probs, scs, seqs = [], [], []
+    rng = np.random.Generator(np.random.PCG64(13))
+    for mm in models:
+        n = len(mm.c)
+        sc = gpu.scale_problem(mm.A, np.zeros(n), mm.l, mm.u, np.where(mm.is_eq, mm.b, -np.inf),
+                               mm.b, bound_objective_rescaling=False)
+        w = np.ones(n)
+        w[mm.int_idx] = sc.D_c[mm.int_idx]
+        probs.append((sc.A, sc.con_ub, mm.is_eq, mm.is_int, sc.var_lb, sc.var_ub, w))
+        scs.append(sc)
+        seq = [np.round(rng.random(n))]
+        for _ in range(args.warmup + args.steps - 1):
+            seq.append(flip_targets(seq[-1], mm.int_idx, mm, rng))
+        seqs.append(seq)
+    params = SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-5,
+                              iteration_limit=2_000_000)
+    nnz = [p[0].nnz for p in probs]
+    ns = [p[0].shape[1] for p in probs]
+    ms = [p[0].shape[0] for p in probs]
+    bytes32 = [16.0 * a + 52.0 * b + 24.0 * c for a, b, c in zip(nnz, ns, ms)]
+    res = {}
+    for precision in (["mixed"] if args.no_fp64 else ["mixed", "fp64"]):
+        t = time.time()
+        bt = gpu.PDFPBatch(probs, precision=precision)
+        log(f"[bench] {precision} batch handle built in {time.time() - t:.1f}s")
+        per = []
+        for s in range(args.warmup + args.steps):
+            if s == args.warmup:
+                barrier(world)
+                clk = ClockSampler(local).__enter__()
+            w0 = time.perf_counter()
+            for p in range(len(probs)):
+                bt.set_target(p, seqs[p][s] / scs[p].D_c)
+            bt.solve(params, 1.0)
+            xs = [bt.get(p, "pdhg_x") for p in range(len(probs))]
+            w1 = time.perf_counter()
+            its = [r["total_count"] for r in bt.results]
+            per.append({"iters": sum(its), "its": its, "device_ms": bt.results[0]["device_ms"],
+                        "wall_s": w1 - w0, "bytes": sum(b * i for b, i in zip(bytes32, its)),
+                        "status": sorted(set(r["status"] for r in bt.results)),
+                        "x_sum": float(sum(np.sum(x) for x in xs))})
+            if s >= args.warmup:
+                log(f"[bench]   {precision} step iters={sum(its)} max={max(its)} "
+                    f"device={per[-1]['device_ms']:.1f}ms status={per[-1]['status']}")
+        clk.__exit__(None, None, None)
+        barrier(world)
+        timed = per[args.warmup:]
+        dev_s = allreduce(world, sum(p["device_ms"] for p in timed) / 1e3, "max")
+        wall_s = allreduce(world, sum(p["wall_s"] for p in timed), "max")
+        iters = allreduce(world, sum(p["iters"] for p in timed), "sum")
+        byts = allreduce(world, sum(p["bytes"] for p in timed), "sum")
+        res[precision] = {"dev_s": dev_s, "wall_s": wall_s, "iters": iters, "bytes": byts,
+                          "clocks": clk.summary(), "steps": timed}
+        bt.close()
+    if rank != 0:
+        return
+    mx = res["mixed"]
+    value = mx["iters"] / mx["dev_s"]
+    peak, peak_kind = measured_hbm_peak()
+    line = {"metric": METRIC, "value": round(value, 1), "unit": "iters/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * mx["dev_s"] / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "batch-uneven: 64 binary covering/packing models, n log-uniform "
+                       "[1000, 200000], m = 0.6 n, 10-40 nnz/row, one batch handle; eps_opt 1e-4, "
+                       "eps_feas 1e-5 per instance", "instances": len(probs), "sum_n": sum(ns),
+                       "sum_m": sum(ms), "sum_nnz": sum(nnz), "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2"},
+            "hbm_gbs": round(mx["bytes"] / mx["dev_s"] / world / 1e9, 1),
+            "hbm_frac": round(mx["bytes"] / mx["dev_s"] / world / 1e9 / peak, 4),
+            "peak_kind": peak_kind,
+            "iterations_per_step": [s["iters"] for s in mx["steps"]],
+            "max_instance_iterations_per_step": [max(s["its"]) for s in mx["steps"]],
+            "e2e": {"value": round(mx["iters"] / mx["wall_s"], 1), "unit": "iters/s",
+                    "h2d_bytes_per_step": 8 * sum(ns), "d2h_bytes_per_step": 8 * sum(ns)},
+            "clocks": mx["clocks"]}
+    if "fp64" in res:
+        fp = res["fp64"]
+        line["fp64_plain"] = {"value": round(fp["iters"] / fp["dev_s"], 1), "unit": "iters/s",
+                              "ms_per_step": round(1e3 * fp["dev_s"] / args.steps, 3),
+                              "hbm_gbs_fp32_bytes": round(fp["bytes"] / fp["dev_s"] / world / 1e9, 1)}
+        line["speedup_vs_fp64_plain"] = round(value / (fp["iters"] / fp["dev_s"]), 3)
+        line["time_speedup_vs_fp64_plain"] = round(fp["dev_s"] / mx["dev_s"], 3)
+    print(json.dumps(line), flush=True)
+
+
+def pump_markshare(args, world, rank):
+    """Time to first feasible of the pump on 32 markshare-shaped models.
+
+    Each model: 6 equality knapsack rows over 50 binaries with U{0..99}
+    coefficients plus 6 slacks in [0, 1000] (model seeds 1..32).  Arms: two
+    trajectories (pump seeds 101 and 201) batched in one projector handle in mixed
+    precision; the same two in FP64; and the plain FP64 single-trajectory pump
+    (seed 101).  Reported: p50/p90 of the wall time to the first feasible point,
+    root LP and handle construction included.  Ranks split the model seeds.
+    """
+    from pdfp_b200 import is_feasible, synthetic
+    from pdfp_b200.pump import feasibility_pump, feasibility_pump_batched
+    seeds = [s for s in range(1, 33) if (s - 1) % world == rank]
+    arms = {"mixed_batched": [], "fp64_batched": [], "fp64_plain": []}
+    found = {k: 0 for k in arms}
+    warm = synthetic.markshare_like(1000)
+    for _ in range(args.warmup):
+        feasibility_pump_batched(warm, seeds=(101, 201), precision="mixed", time_limit=60)
+        feasibility_pump(warm, seed=101, precision="fp64", time_limit=60)
+    for s in seeds:
+        m = synthetic.markshare_like(s)
+        t = time.perf_counter()
+        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="mixed", time_limit=60)
+        arms["mixed_batched"].append(time.perf_counter() - t)
+        found["mixed_batched"] += int(r.found and is_feasible(m, r.x))
+        t = time.perf_counter()
+        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="fp64", time_limit=60)
+        arms["fp64_batched"].append(time.perf_counter() - t)
+        found["fp64_batched"] += int(r.found and is_feasible(m, r.x))
+        t = time.perf_counter()
+        r = feasibility_pump(m, seed=101, precision="fp64", time_limit=60)
+        arms["fp64_plain"].append(time.perf_counter() - t)
+        found["fp64_plain"] += int(r.found and is_feasible(m, r.x))
+    if world > 1:
+        import torch.distributed as dist
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (arms, found))
+        arms = {k: sum((g[0][k] for g in gathered), []) for k in arms}
+        found = {k: sum(g[1][k] for g in gathered) for k in found}
+    if rank != 0:
+        return
+
+    def pct(v, q):
+        return round(1e3 * float(np.percentile(v, q)), 2)
+
+    out = {k: {"p50_ms": pct(v, 50), "p90_ms": pct(v, 90), "found": found[k], "runs": len(v)}
+           for k, v in arms.items()}
+    from oracle import oracle as O
+    cpu = []
+    for s in range(1, 9):
+        m = synthetic.markshare_like(s)
+        t = time.perf_counter()
+        feasibility_pump_batched(m, seeds=(101, 201), solvers=O.OracleSolvers(), time_limit=60)
+        cpu.append(time.perf_counter() - t)
+    line = {"metric": "time to first feasible, pump with 2 batched trajectories",
+            "value": out["mixed_batched"]["p50_ms"], "unit": "ms (p50)", "n_gpus": world,
+            "steps": len(arms["mixed_batched"]), "warmup": args.warmup,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "pump-markshare: 6 equality rows x (50 binaries + 6 slacks in "
+                       "[0,1000]), U{0..99} coefficients, b = floor(rowsum/2), model seeds 1..32, "
+                       "pump seeds 101 and 201"},
+            "arms": out,
+            "p90_speedup_vs_fp64_plain": round(out["fp64_plain"]["p90_ms"]
+                                               / max(out["mixed_batched"]["p90_ms"], 1e-9), 3),
+            "cpu_baseline": {"value": round(1e3 * float(np.median(cpu)), 2), "unit": "ms (p50)",
+                             "cores": 1, "kind": "port",
+                             "sample": "the same batched pump on the CPU oracle, model seeds 1..8"}}
+    print(json.dumps(line), flush=True)
 
 
 def reference_arm(args, world, rank):

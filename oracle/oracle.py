@@ -332,3 +332,35 @@ class OracleSolvers:
     @staticmethod
     def PDFPState(A, b, is_eq, is_int, var_lb, var_ub, w, precision="fp64"):
         return _OracleProjector(A, b, is_eq, is_int, var_lb, var_ub, w)
+
+    class PDFPBatch:
+        """Independent oracle projectors behind the batch interface."""
+
+        def __init__(self, problems, precision="fp64"):
+            self.members = []
+            for pr in problems:
+                s = _OracleProjector(*pr[:7])
+                if len(pr) > 7 and pr[7] is not None:
+                    s.original_primal_residual(1.0 / np.asarray(pr[7]))
+                self.members.append(s)
+            self.results = [None] * len(self.members)
+
+        def set_x(self, p, x):
+            self.members[p].set_x(x)
+
+        def set_target(self, p, xt):
+            self.members[p].set_target(xt)
+
+        def warm_start(self, p):
+            self.members[p].warm_start()
+
+        def solve(self, params, primal_weights):
+            pws = np.broadcast_to(np.asarray(primal_weights, dtype=float), (len(self.members),))
+            out = []
+            for p, s in enumerate(self.members):
+                out.append(s.solve(params[p], float(pws[p])))
+                self.results[p] = dict(s.last)
+            return out
+
+        def get(self, p, which):
+            return self.members[p].get(which)

@@ -11,8 +11,9 @@ pdfp_b200.gpu); rounding and propagation run on the CPU.
 """
 from .milp import MILP, is_feasible, max_violation, num_constraints, num_continuous, num_variables, read_mps, write_solution
 from .params import RestartParameters, SolverParameters
-from .pump import PumpResult, feasibility_pump
+from .pump import PumpResult, TrajectoryResult, feasibility_pump, feasibility_pump_batched
 
 __all__ = ["MILP", "read_mps", "max_violation", "is_feasible", "write_solution", "num_variables",
            "num_constraints", "num_continuous", "feasibility_pump", "PumpResult",
+           "feasibility_pump_batched", "TrajectoryResult",
            "SolverParameters", "RestartParameters"]

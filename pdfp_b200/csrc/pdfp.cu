@@ -452,8 +452,11 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     for (auto& e : tev_) PDFP_CK(cudaEventCreate(&e));
     for (auto& e : sev_) PDFP_CK(cudaEventCreate(&e));
     PDFP_CK(cudaDeviceSynchronize());
+    // The autotuner pays for itself only where a step kernel takes longer than its
+    // launch: below 256K nonzeros every candidate times the same few microseconds.
+    // PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size.
     const char* at = std::getenv("PDFP_AUTOTUNE");
-    const bool tune = !(at && at[0] == '0');
+    const bool tune = at && at[0] == '0' ? false : (at && at[0] == '1' ? true : M_.L.NNZ >= (1 << 18));
     if (precision_ == PDFP_MIXED) {
         if (tune) autotune(true); else { prepare_side(p32_, true, true); prepare_side(d32_, false, true); }
     }

@@ -8,7 +8,8 @@
 // scaling factors and scaled values are bit-identical to the reference's CPU
 // arithmetic (Julia walks its CSC matrix column by column, which gives each row
 // sum its terms in ascending column order and each column sum in ascending row
-// order).  The two norms of the optional rescaling are tree reductions.
+// order).  The scaled bounds, costs and the optional bound/objective rescaling
+// (two sequential norms, as the reference's loops) run on the device too.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -68,6 +69,74 @@ __global__ void mul_inplace_kernel(double* __restrict__ d, const double* __restr
         d[i] = __dmul_rn(d[i], s[i]);
 }
 
+// scaled bounds and costs, src/preconditioner.jl:66-70:
+// c_s = c .* D_c; var bounds / D_c and row bounds .* D_r where finite
+__global__ void scale_vectors_kernel(const double* __restrict__ c, const double* __restrict__ lb,
+                                     const double* __restrict__ ub, const double* __restrict__ D_c,
+                                     int32_t n, const double* __restrict__ clb,
+                                     const double* __restrict__ cub, const double* __restrict__ D_r,
+                                     int32_t m, double* __restrict__ c_s, double* __restrict__ lb_s,
+                                     double* __restrict__ ub_s, double* __restrict__ clb_s,
+                                     double* __restrict__ cub_s) {
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        c_s[j] = __dmul_rn(c[j], D_c[j]);
+        lb_s[j] = isfinite(lb[j]) ? lb[j] / D_c[j] : lb[j];
+        ub_s[j] = isfinite(ub[j]) ? ub[j] / D_c[j] : ub[j];
+    }
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        clb_s[i] = isfinite(clb[i]) ? __dmul_rn(clb[i], D_r[i]) : clb[i];
+        cub_s[i] = isfinite(cub[i]) ? __dmul_rn(cub[i], D_r[i]) : cub[i];
+    }
+}
+
+// bound/objective rescaling, src/preconditioner.jl:72-96: the two squared
+// norms (sequential sums, as the reference's loops), then the scaling
+__global__ void rescale_norms_kernel(const double* __restrict__ clb, const double* __restrict__ cub,
+                                     const double* __restrict__ clb_s,
+                                     const double* __restrict__ cub_s, int32_t m,
+                                     const double* __restrict__ c_s, int32_t n,
+                                     double* __restrict__ out /* bound_sq, c_sq */) {
+    if (threadIdx.x == 0) {
+        double bound_sq = 0.0;
+        for (int32_t i = 0; i < m; ++i) {
+            const bool flo = isfinite(clb[i]), fhi = isfinite(cub[i]);
+            const double lo = clb_s[i], hi = cub_s[i];
+            if (flo && (!fhi || fabs(lo - hi) > SCALING_EPSILON)) bound_sq = __dadd_rn(bound_sq, __dmul_rn(lo, lo));
+            if (fhi) bound_sq = __dadd_rn(bound_sq, __dmul_rn(hi, hi));
+        }
+        out[0] = bound_sq;
+    }
+    if (threadIdx.x == 32) {
+        double c_sq = 0.0;
+        for (int32_t j = 0; j < n; ++j) c_sq = __dadd_rn(c_sq, __dmul_rn(c_s[j], c_s[j]));
+        out[1] = c_sq;
+    }
+}
+
+__global__ void rescale_apply_kernel(const double* __restrict__ lb, const double* __restrict__ ub,
+                                     int32_t n, const double* __restrict__ clb,
+                                     const double* __restrict__ cub, int32_t m,
+                                     const double* __restrict__ sq, double* __restrict__ c_s,
+                                     double* __restrict__ lb_s, double* __restrict__ ub_s,
+                                     double* __restrict__ clb_s, double* __restrict__ cub_s,
+                                     double* __restrict__ scales /* bound, objective */) {
+    const double bs = 1.0 / (sqrt(sq[0]) + 1.0);
+    const double os = 1.0 / (sqrt(sq[1]) + 1.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scales[0] = bs;
+        scales[1] = os;
+    }
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (isfinite(clb[i])) clb_s[i] = __dmul_rn(clb_s[i], bs);
+        if (isfinite(cub[i])) cub_s[i] = __dmul_rn(cub_s[i], bs);
+    }
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        if (isfinite(lb[j])) lb_s[j] = __dmul_rn(lb_s[j], bs);
+        if (isfinite(ub[j])) ub_s[j] = __dmul_rn(ub_s[j], bs);
+        c_s[j] = __dmul_rn(c_s[j], os);
+    }
+}
+
 static int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8192))); }
 
 void scale_problem_device(const pdfp_csr& A, const double* c, const double* var_lb,
@@ -110,48 +179,37 @@ void scale_problem_device(const pdfp_csr& A, const double* c, const double* var_
     PDFP_CK(cudaGetLastError());
     PDFP_CK(cudaDeviceSynchronize());
 
+    // scaled vectors and the optional bound/objective rescaling, on the device
     const int64_t nnz = M.L.NNZ;
-    std::vector<double> hDr(m), hDc(n);
-    if (m) PDFP_CK(cudaMemcpy(hDr.data(), D_r, sizeof(double) * m, cudaMemcpyDeviceToHost));
-    if (n) PDFP_CK(cudaMemcpy(hDc.data(), D_c, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    double* dv[10];
+    const double* hin[5] = {c, var_lb, var_ub, con_lb, con_ub};
+    const int64_t len[5] = {n, n, n, m, m};
+    for (int k = 0; k < 5; ++k) {
+        dv[k] = ar.alloc<double>(len[k]);
+        if (len[k]) PDFP_CK(cudaMemcpy(dv[k], hin[k], sizeof(double) * len[k], cudaMemcpyHostToDevice));
+    }
+    for (int k = 5; k < 10; ++k) dv[k] = ar.alloc<double>(len[k - 5]);
+    double* sq = ar.alloc<double>(4);
+    const int bb = blocks_for(std::max(m, n));
+    scale_vectors_kernel<<<bb, 256>>>(dv[0], dv[1], dv[2], D_c, n, dv[3], dv[4], D_r, m, dv[5],
+                                      dv[6], dv[7], dv[8], dv[9]);
+    double scales[2] = {1.0, 1.0};
+    if (rescale) {
+        rescale_norms_kernel<<<1, 64>>>(dv[3], dv[4], dv[8], dv[9], m, dv[5], n, sq);
+        rescale_apply_kernel<<<bb, 256>>>(dv[1], dv[2], n, dv[3], dv[4], m, sq, dv[5], dv[6], dv[7],
+                                          dv[8], dv[9], sq + 2);
+    }
+    PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaDeviceSynchronize());
+    if (rescale) PDFP_CK(cudaMemcpy(scales, sq + 2, sizeof(scales), cudaMemcpyDeviceToHost));
     if (nnz) PDFP_CK(cudaMemcpy(val_out, M.v64_a, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
-    // scaled vectors, src/preconditioner.jl:66-70
-    for (int32_t j = 0; j < n; ++j) {
-        c_out[j] = c[j] * hDc[j];
-        var_lb_out[j] = std::isfinite(var_lb[j]) ? var_lb[j] / hDc[j] : var_lb[j];
-        var_ub_out[j] = std::isfinite(var_ub[j]) ? var_ub[j] / hDc[j] : var_ub[j];
-        D_c_out[j] = hDc[j];
-    }
-    for (int32_t i = 0; i < m; ++i) {
-        con_lb_out[i] = std::isfinite(con_lb[i]) ? con_lb[i] * hDr[i] : con_lb[i];
-        con_ub_out[i] = std::isfinite(con_ub[i]) ? con_ub[i] * hDr[i] : con_ub[i];
-        D_r_out[i] = hDr[i];
-    }
-    double bs = 1.0, os = 1.0;
-    if (rescale) {  // src/preconditioner.jl:72-96
-        double bound_sq = 0.0;
-        for (int32_t i = 0; i < m; ++i) {
-            const bool flo = std::isfinite(con_lb[i]), fhi = std::isfinite(con_ub[i]);
-            const double lo = con_lb_out[i], hi = con_ub_out[i];
-            if (flo && (!fhi || std::fabs(lo - hi) > SCALING_EPSILON)) bound_sq += lo * lo;
-            if (fhi) bound_sq += hi * hi;
-        }
-        double csq = 0.0;
-        for (int32_t j = 0; j < n; ++j) csq += c_out[j] * c_out[j];
-        bs = 1.0 / (std::sqrt(bound_sq) + 1.0);
-        os = 1.0 / (std::sqrt(csq) + 1.0);
-        for (int32_t i = 0; i < m; ++i) {
-            if (std::isfinite(con_lb[i])) con_lb_out[i] *= bs;
-            if (std::isfinite(con_ub[i])) con_ub_out[i] *= bs;
-        }
-        for (int32_t j = 0; j < n; ++j) {
-            if (std::isfinite(var_lb[j])) var_lb_out[j] *= bs;
-            if (std::isfinite(var_ub[j])) var_ub_out[j] *= bs;
-            c_out[j] *= os;
-        }
-    }
-    *bound_scale = bs;
-    *objective_scale = os;
+    double* hout[7] = {c_out, var_lb_out, var_ub_out, con_lb_out, con_ub_out, D_c_out, D_r_out};
+    const double* dsrc[7] = {dv[5], dv[6], dv[7], dv[8], dv[9], D_c, D_r};
+    const int64_t olen[7] = {n, n, n, m, m, n, m};
+    for (int k = 0; k < 7; ++k)
+        if (olen[k]) PDFP_CK(cudaMemcpy(hout[k], dsrc[k], sizeof(double) * olen[k], cudaMemcpyDeviceToHost));
+    *bound_scale = scales[0];
+    *objective_scale = scales[1];
 }
 
 double estimate_sv_device(const pdfp_csr& A, int32_t max_iterations, double tolerance,

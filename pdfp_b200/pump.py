@@ -400,3 +400,210 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
             _print_iteration(iteration, distance, violation, inner, gap_used, action, elapsed())
     found = max_violation(milp, xt) <= tol and is_integral(xt, int_idx, tol)
     return _finish(milp, found, xt, stats, elapsed(), verbose)
+
+
+@dataclass
+class TrajectoryResult:
+    """One trajectory of a batched pump run."""
+
+    seed: int
+    found: bool
+    iterations: int
+    perturbations: int
+    pdhg_iterations: int
+    time_to_feasible: float
+
+
+class _Trajectory:
+    """The CPU-side state of one pump trajectory (src/pump.jl:262-316)."""
+
+    def __init__(self, milp, seed, x, dual_slack, push_threshold, violation_threshold,
+                 propagation_budget, swap_iteration, batch_policy, flip_parameter, mixed):
+        n = num_variables(milp)
+        self.seed = seed
+        self.rng = np.random.Generator(np.random.PCG64(seed))
+        self.rounder = Rounder(milp, max_pops=(2**62 if mixed else propagation_budget),
+                               swap_iteration=swap_iteration,
+                               policy=BatchPolicy() if batch_policy == "cost" else None)
+        self.rounder.schedule = _batch_schedule(milp, x, dual_slack, push_threshold)
+        self.xt = round_guarded(self.rounder, x, self.rng, 0)
+        if _total_integer_row_violation(milp, self.xt) >= violation_threshold:
+            direction = [False] * n
+            for j in milp.int_idx.tolist():
+                direction[j] = True
+            self.rounder.direction = direction
+        self.general = [j for j in milp.int_idx.tolist() if not (milp.l[j] == 0.0 and milp.u[j] == 1.0)]
+        self.is_general = np.zeros(n, dtype=bool)
+        self.is_general[self.general] = True
+        self.ladder = RestartLadder(0.0, 0, flip_parameter, max(len(self.general) // 10, 10))
+        self.seen: set = set()
+        self.h_current = _hash_integers(self.xt, milp.int_idx)
+        self.since_restart = 0
+        self.iterations = 0
+        self.perturbations = 0
+        self.pdhg = 0
+        self.found = False
+        self.x_found = None
+        self.t_found = math.inf
+
+
+def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float = 1800.0,
+                             flip_parameter: int = 20, restart_period: int = 100,
+                             swap_iteration: int = 10, gap_start: float = 1e-2,
+                             gap_decay: float = 0.98, gap_floor: float = 1e-4,
+                             residual_ratio: float = 0.1, root_lp_tolerance: float = 1e-2,
+                             projection_iteration_limit: int = 500_000, batch_policy: str = "cost",
+                             push_threshold: float = 0.01, violation_threshold: float = 5000.0,
+                             propagation_budget: int = 100_000,
+                             feasibility_tolerance: float = 1e-6, precision: str = "fp64",
+                             solvers=None, stop=None):
+    """Concurrent pump trajectories as members of one batched projector.
+
+    Replaces the reference's K concurrent pump processes (scripts/solve.jl:121-148,
+    seeds 100k + seed) with K trajectories in one process: one root LP, one
+    scaling, and per pump iteration one batched projection (one launch sequence
+    for all trajectories, each with its own restart and termination state on the
+    device).  Rounding, flips and restarts run per trajectory on the CPU with the
+    reference's rules (src/pump.jl:320-406).  Returns (PumpResult of the first
+    trajectory to find a feasible point -- or of trajectory 0 if none did --,
+    list of TrajectoryResult).
+
+    ``stop(done) -> bool``, when given, is called once at the head of every pump
+    iteration with this process's own verdict (a trajectory succeeded or the time
+    ran out) and decides whether to stop; the sharded driver uses it to agree on
+    stopping across ranks.
+    """
+    if batch_policy not in ("cost", "always"):
+        raise ValueError("batch_policy must be 'cost' or 'always'")
+    if len(seeds) < 1:
+        raise ValueError("at least one trajectory seed is required")
+    if solvers is None:
+        from . import gpu as solvers  # noqa: PLC0415
+    t0 = time.time()
+
+    def elapsed():
+        return time.time() - t0
+
+    def remaining():
+        return max(time_limit - elapsed(), 1.0)
+
+    n, m = num_variables(milp), num_constraints(milp)
+    int_idx = milp.int_idx
+    tol = feasibility_tolerance
+    mixed = num_continuous(milp) > 0
+    stats = PumpCounters()
+    x, dual_slack, stats.root_lp_status, _ = solvers.solve_lp_relaxation(
+        milp, tolerance=root_lp_tolerance, time_limit=remaining(), cupdlpx_termination=mixed)
+    stats.root_lp_time = elapsed()
+    K = len(seeds)
+    if is_integral(x, int_idx, tol):
+        xt = _round_to_nearest(x, milp)
+        if max_violation(milp, xt) <= tol:
+            res = _finish(milp, True, xt, stats, elapsed(), False)
+            return res, [TrajectoryResult(s, True, 0, 0, 0, elapsed()) for s in seeds]
+    trajs = [_Trajectory(milp, s, x, dual_slack, push_threshold, violation_threshold,
+                         propagation_budget, swap_iteration, batch_policy, flip_parameter, mixed)
+             for s in seeds]
+    is_eq, is_int = milp.is_eq, milp.is_int
+    con_lb = np.where(is_eq, milp.b, -np.inf)
+    sp_ = solvers.scale_problem(milp.A, np.zeros(n), milp.l.copy(), milp.u.copy(), con_lb,
+                                milp.b.copy(), bound_objective_rescaling=False)
+    D_c = sp_.D_c
+    weights = np.ones(n)
+    weights[int_idx] = D_c[int_idx]
+    ru = (1.0 / sp_.D_r) if mixed else None
+    prob = (sp_.A, sp_.con_ub, is_eq, is_int, sp_.var_lb, sp_.var_ub, weights, ru)
+    batch = solvers.PDFPBatch([prob] * K, precision=precision)
+    for p in range(K):
+        batch.set_x(p, x / D_c)
+    primal_weight = math.sqrt(1.0 + (len(int_idx) / m if m > 0 else 0.0))
+    gaps = [gap_start] * K
+    budgets = [gap_start] * K
+
+    def params_for(p, active):
+        return SolverParameters(iteration_limit=projection_iteration_limit if active else 0,
+                                eps_optimal_relative=gaps[p],
+                                eps_feasible_relative=gaps[p] * residual_ratio,
+                                time_limit=remaining())
+
+    winner = None
+    while True:
+        done = winner is not None or elapsed() >= time_limit
+        if (stop(done) if stop is not None else done):
+            break
+        for p, tr in enumerate(trajs):
+            if max_violation(milp, tr.xt) <= tol and is_integral(tr.xt, int_idx, tol):
+                tr.found, tr.x_found, tr.t_found = True, tr.xt.copy(), elapsed()
+                winner = p
+                break
+        if winner is not None:
+            continue
+        for p, tr in enumerate(trajs):
+            tr.iterations += 1
+            tr.since_restart += 1
+            batch.set_target(p, tr.xt / D_c)
+        t = time.time()
+        batch.solve([params_for(p, True) for p in range(K)], primal_weight)
+        xs = [D_c * batch.get(p, "pdhg_x") for p in range(K)]
+        inner = [batch.results[p]["total_count"] for p in range(K)]
+        # mixed models: tenfold tighter re-solves (src/pump.jl:343-356), batched
+        while mixed and elapsed() < time_limit:
+            need = [p for p in range(K) if budgets[p] > 1e-6 and is_integral(xs[p], int_idx, tol)
+                    and max_violation(milp, _round_to_nearest(xs[p], milp)) > tol]
+            if not need:
+                break
+            for p in need:
+                budgets[p] *= 0.1
+                gaps[p] = max(gaps[p] * 0.1, 1e-8)
+                batch.warm_start(p)
+            batch.solve([params_for(p, p in need) for p in range(K)], primal_weight)
+            for p in need:
+                xs[p] = D_c * batch.get(p, "pdhg_x")
+                inner[p] += batch.results[p]["total_count"]
+        stats.projection_time += time.time() - t
+        for p, tr in enumerate(trajs):
+            tr.pdhg += inner[p]
+            if gaps[p] > gap_floor:
+                gaps[p] = max(gaps[p] * gap_decay, gap_floor)
+            xp = xs[p]
+            if is_integral(xp, int_idx, tol):
+                cand = _round_to_nearest(xp, milp)
+                if max_violation(milp, cand) <= tol:
+                    tr.found, tr.x_found, tr.t_found = True, cand, elapsed()
+                    winner = p
+                    break
+            t = time.time()
+            x_round = round_guarded(tr.rounder, xp, tr.rng, tr.iterations)
+            stats.rounding_time += time.time() - t
+            candidate = tr.xt.copy()
+            if _differs(x_round, tr.xt, int_idx):
+                candidate[:] = x_round
+            else:
+                flips = int(tr.rng.integers(flip_parameter // 2, 3 * flip_parameter // 2 + 1))
+                _flip_farthest(candidate, xp, milp, flips)
+            h_candidate = _hash_integers(candidate, int_idx)
+            cycled = h_candidate in tr.seen
+            periodic = tr.since_restart >= restart_period
+            if cycled or periodic:
+                _perturb(candidate, xp, milp, tr.rng, tr.general, tr.is_general, tr.ladder,
+                         tr.iterations)
+                tr.perturbations += 1
+                tr.since_restart = 0
+                for _ in range(10):
+                    h = _hash_integers(candidate, int_idx)
+                    if not (h in tr.seen or h == tr.h_current):
+                        break
+                    _perturb(candidate, xp, milp, tr.rng, tr.general, tr.is_general, tr.ladder,
+                             tr.iterations)
+            tr.seen.add(tr.h_current)
+            tr.h_current = _hash_integers(candidate, int_idx) if (cycled or periodic) else h_candidate
+            tr.xt = candidate
+    best = trajs[winner] if winner is not None else trajs[0]
+    stats.iterations = best.iterations
+    stats.perturbations = best.perturbations
+    stats.pdhg_iterations = best.pdhg
+    xbest = best.x_found if best.found else best.xt
+    found = best.found or (max_violation(milp, xbest) <= tol and is_integral(xbest, int_idx, tol))
+    res = _finish(milp, found, xbest, stats, elapsed(), False)
+    return res, [TrajectoryResult(tr.seed, tr.found, tr.iterations, tr.perturbations, tr.pdhg,
+                                  tr.t_found) for tr in trajs]

@@ -40,3 +40,23 @@ def test_p0201_first_iteration_matches_published_log(examples, capsys):
     assert float(first[1]) == pytest.approx(it1["distance"], rel=1e-5)
     assert int(first[2]) == it1["violation"] and int(first[3]) == it1["pdhg"]
     assert any(l.startswith("device      NVIDIA") for l in out)
+
+
+@pytest.mark.parametrize("name", ["pk1", "gen-ip054"])
+def test_pump_fp64_takes_the_oracle_pumps_steps(examples, oracle, name):
+    """With the deterministic rounding policy the FP64 GPU pump and the pump on the
+    oracle's solvers take the same steps and return the same point.
+
+    p0201 is left out: it has identical columns, whose LP values are equal in exact
+    arithmetic, so the rounder's order among them -- and from the second pump
+    iteration on the whole trajectory -- follows last-bit differences between the
+    GPU's and the oracle's FP64 sums (the first iteration still matches the
+    published log, tested above)."""
+    m = examples[name]
+    r_o = feasibility_pump(m, time_limit=120.0, solvers=oracle.OracleSolvers(), seed=3,
+                           batch_policy="always")
+    r_g = feasibility_pump(m, time_limit=120.0, precision="fp64", seed=3, batch_policy="always")
+    assert (r_g.found, r_g.iterations, r_g.perturbations) == (r_o.found, r_o.iterations,
+                                                             r_o.perturbations)
+    assert r_g.pdhg_iterations == r_o.pdhg_iterations
+    assert np.array_equal(r_g.x, r_o.x)
