@@ -203,6 +203,22 @@ def run_projections(state, sc, xt_seq, params, timed):
     return out
 
 
+def time_reference_form(sc, w, xt0, is_eq, is_int, warm=20, timed=200):
+    """PDHG steps/s of the reference's own GPU step structure on the same problem:
+    cuSPARSE SpMV with A', primal kernel, dual_y kernel, cuSPARSE SpMV with A, dual_z
+    kernel, FP64 (src/pdfp_kernels.jl).  Steps only: no evaluation is charged to it."""
+    from pdfp_b200 import refform
+    r = refform.RefFormState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w)
+    r.reset(xt0 / sc.D_c, np.zeros(len(xt0)))
+    step = 0.998 / np.sqrt(2.0)
+    r.steps(step, 1.0, 1, warm)
+    ms = r.steps(step, 1.0, 1 + warm, timed)
+    r.close()
+    return {"value": round(timed / (ms * 1e-3), 1), "unit": "iters/s",
+            "ms_per_iter": round(ms / timed, 5), "launches_per_iter": 5,
+            "note": "steps only (no evaluation windows), FP64, cuSPARSE SpMV"}
+
+
 def cpu_baseline(sc, w, xt0, is_eq, is_int, threads, iterations, label):
     """The oracle's PDHG steps on the same scaled problem: iterations/s on `threads` host threads."""
     from oracle import oracle as O
@@ -233,6 +249,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iterations", type=int, default=40)
+    ap.add_argument("--no-refform", action="store_true",
+                    help="skip the reference-structured FP64 step (cuSPARSE + 3 kernels)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -294,6 +312,10 @@ def main():
                               "kd_ms": float(np.mean(kd)) if kd else None}
         del st
 
+    refform_line = None
+    if not args.no_refform:
+        refform_line = time_reference_form(sc, w, xt0, is_eq, is_int)
+        log(f"[bench] reference form (FP64, cuSPARSE + 3 kernels): {refform_line}")
     if rank != 0:
         barrier(world)
         return
@@ -339,6 +361,9 @@ def main():
                               "kernel_primal_ms": fp["kp_ms"]}
         line["speedup_vs_fp64_plain"] = round(value / fv, 3)
         line["time_speedup_vs_fp64_plain"] = round(fp["dev_s"] / mx["dev_s"], 3)
+    if refform_line is not None:
+        line["fp64_reference_form"] = refform_line
+        line["speedup_vs_fp64_reference_form"] = round(value / refform_line["value"], 3)
     line["roofline"] = roof
     h2d = 8 * n * args.steps
     line["e2e"] = {"value": round(mx["tot_iters"] / mx["wall_s"], 1), "unit": "iters/s",

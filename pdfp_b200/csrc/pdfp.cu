@@ -29,6 +29,7 @@ namespace pdfp {
 
 constexpr int NT_EVAL = 256;
 constexpr int STALL_EVALS = 10;  // evaluations without 10% KKT progress before the FP64 polish
+constexpr double kFp32TolFloor = 1e-6;  // tighter relative tolerances run in FP64 from the start
 
 // ---- per-instance state kernels ---------------------------------------------------
 
@@ -831,7 +832,11 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         s.primal_weight = primal_weights[p];
         s.iter_limit = q.iteration_limit;
         s.freq = q.termination_evaluation_frequency;
-        s.mode = precision_ == PDFP_MIXED ? MODE_FP32 : MODE_FP64;
+        // FP32 iterates carry about seven significant digits: a mixed handle runs an
+        // instance whose tolerance asks for more (below kFp32TolFloor) in FP64 from
+        // the start instead of reaching the FP64 polish through a stall.
+        const bool tight = std::min(q.eps_optimal_relative, q.eps_feasible_relative) < kFp32TolFloor;
+        s.mode = precision_ == PDFP_MIXED && !tight ? MODE_FP32 : MODE_FP64;
         sv_it = q.sv_max_iterations;
         sv_tol = q.sv_tolerance;
         max_time = std::max(max_time, q.time_limit);
@@ -840,14 +845,20 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     solve_begin_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, K_);
     PDFP_CK(cudaGetLastError());
     ensure_step_sizes(sv_it, sv_tol);
-    // a mixed handle starts every solve in FP32: bring back instances a polish left in FP64
+    // a mixed handle starts each instance in the mode chosen above: convert the
+    // iterates of instances whose vectors are in the other form
+    bool with32 = false, with64 = false;
+    for (int p = 0; p < K_; ++p) (sp[p].mode == MODE_FP32 ? with32 : with64) = true;
     if (precision_ == PDFP_MIXED) {
         const HostLayout& L = M_.L;
         for (int p = 0; p < K_; ++p) {
-            if (vec_mode_[p] != MODE_FP64) continue;
+            if (vec_mode_[p] == sp[p].mode) continue;
             const int64_t len = (L.col_off[p + 1] - L.col_off[p]) + (L.row_off[p + 1] - L.row_off[p]);
-            launch_elem(K_, len, ConvertVecs<double, float>{v64_, v32_, M_.col_off, M_.row_off, p}, stream_);
-            vec_mode_[p] = MODE_FP32;
+            if (sp[p].mode == MODE_FP32)
+                launch_elem(K_, len, ConvertVecs<double, float>{v64_, v32_, M_.col_off, M_.row_off, p}, stream_);
+            else
+                launch_elem(K_, len, ConvertVecs<float, double>{v32_, v64_, M_.col_off, M_.row_off, p}, stream_);
+            vec_mode_[p] = sp[p].mode;
         }
     }
     PDFP_CK(cudaMemcpyAsync(sp_, sp.data(), sizeof(SolveParams) * K_, cudaMemcpyHostToDevice, stream_));
@@ -857,8 +868,6 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     PDFP_CK(cudaGetLastError());
     PDFP_CK(cudaMemsetAsync(err_, 0, sizeof(int32_t) * 4, stream_));
 
-    bool with32 = precision_ == PDFP_MIXED;
-    bool with64 = precision_ != PDFP_MIXED;
     // first poll: instances may already be done (iteration_limit <= total)
     PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
     PDFP_CK(cudaStreamSynchronize(stream_));
