@@ -365,6 +365,20 @@ def main():
         line["fp64_reference_form"] = refform_line
         line["speedup_vs_fp64_reference_form"] = round(value / refform_line["value"], 3)
     line["roofline"] = roof
+    if mx["kp_ms"]:
+        # the ceiling that binds a scattered sparsity pattern: random 4-byte gathers
+        grate = gpu.C.c_double()
+        gpu.L.check(gpu.L.lib().pdfp_measure_gather_rate((nnz // 4) * 4, m, 20, gpu.C.byref(grate)))
+        peak_g = grate.value / 1e9
+        ach_p = nnz / (mx["kp_ms"] * 1e-3) / 1e9
+        ach_d = nnz / (mx["kd_ms"] * 1e-3) / 1e9 if mx["kd_ms"] else None
+        line["gather_roofline"] = {
+            "bound": "random 4-byte gathers", "unit": "Ggathers/s", "peak": round(peak_g, 1),
+            "achieved": round(ach_p, 1), "frac": round(ach_p / peak_g, 4),
+            "dual_kernel_achieved": round(ach_d, 1) if ach_d else None,
+            "dual_kernel_frac": round(ach_d / peak_g, 4) if ach_d else None,
+            "peak_source": "pdfp_measure_gather_rate on this GPU (streamed indices, "
+                           f"{(nnz // 4) * 4} gathers from a {m}-entry FP32 vector)"}
     h2d = 8 * n * args.steps
     line["e2e"] = {"value": round(mx["tot_iters"] / mx["wall_s"], 1), "unit": "iters/s",
                    "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,

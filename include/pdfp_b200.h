@@ -181,15 +181,20 @@ PDFP_API int pdfp_destroy(pdfp_handle* h);
  * reports their mean durations (benchmark support; off by default). */
 PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
 
-/* The step-kernel configuration the autotuner chose at creation (it times
- * every candidate shared-memory stage size x block size on the handle's own
- * matrix; set PDFP_AUTOTUNE=0 to use the default): out[8] = {A' stage bytes,
- * A' threads per role, A' tiles, A stage bytes, A threads per role, A tiles,
+/* The step-kernel configuration the autotuner chose at creation.  It times, on
+ * the handle's own matrix, the tile engine (shared-memory stage size x threads
+ * per role x gather cache policy) and the flat engine (both cache policies) and
+ * keeps the fastest per side; below 256K nonzeros it keeps the default.
+ * PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size, and
+ * PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the engine with its default
+ * settings (flat1: the flat engine's one-quad-per-thread variant).
+ * out[8] = {A' stage bytes, A' threads per role (0: flat engine), A' tiles,
+ * A stage bytes, A threads per role (0: flat engine), A tiles,
  * A' gathers L2-only, A gathers L2-only}. */
 PDFP_API int pdfp_get_tuning(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
  * launch time, cfg[4i..4i+3] = {side (0: A', 1: A), stage bytes, threads per
- * role, gathers L2-only}; *count receives the number of rows. */
+ * role (0: flat engine), gathers L2-only}; *count receives the number of rows. */
 PDFP_API int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
                                    int32_t* count);
 
@@ -211,6 +216,16 @@ PDFP_API int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double
                        double* var_lb_out, double* var_ub_out, double* con_lb_out,
                        double* con_ub_out, double* D_r, double* D_c, double* bound_scale,
                        double* objective_scale);
+
+/* Measurement support (no counterpart in the reference): the rate, in gathers
+ * per second, at which this GPU serves `nnz` independent random 4-byte loads
+ * from an m-entry FP32 vector when indices and values stream in coalesced --
+ * the ceiling of a sparse step whose column indices are scattered, measured
+ * with the simplest kernel that reaches it (best of `repeats` launches in a
+ * few launch shapes).  nnz: a positive multiple of 4 below 2^31.  Allocates
+ * and frees its own test data. */
+PDFP_API int pdfp_measure_gather_rate(int64_t nnz, int32_t m, int32_t repeats,
+                                      double* gathers_per_s);
 
 /* estimate_max_singular_value(A, A_t, m; max_iterations, tolerance),
  * src/preconditioner.jl:108-125, on the device. */

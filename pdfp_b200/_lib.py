@@ -109,6 +109,7 @@ SIGNATURES = {
     "pdfp_scale_problem": (C.c_int, [C.POINTER(Csr), dp, dp, dp, dp, dp, C.c_int32, C.c_double,
                                      C.c_int32, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]),
     "pdfp_estimate_max_singular_value": (C.c_int, [C.POINTER(Csr), C.c_int32, C.c_double, dp, ip]),
+    "pdfp_measure_gather_rate": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, dp]),
     "pdfp_estimate_max_singular_value_noalloc": (C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, ip,
                                                             ip, dp, C.c_int32, C.c_double,
                                                             C.c_void_p, dp, ip]),

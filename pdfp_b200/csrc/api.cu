@@ -245,6 +245,14 @@ int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double* var_lb,
     });
 }
 
+int pdfp_measure_gather_rate(int64_t nnz, int32_t m, int32_t repeats, double* gathers_per_s) {
+    return guarded([&] {
+        if (!gathers_per_s) throw pdfp::Error(PDFP_E_INVALID, "null output");
+        require_device();
+        *gathers_per_s = pdfp::measure_gather_rate(nnz, m, repeats);
+    });
+}
+
 int pdfp_estimate_max_singular_value(const pdfp_csr* A, int32_t max_iterations, double tolerance,
                                      double* sigma, int32_t* iterations) {
     return guarded([&] {

@@ -8,6 +8,7 @@
 #include "common.cuh"
 #include "layout.hpp"
 #include "state.hpp"
+#include "flat_spmv.cuh"
 #include "tile_spmv.cuh"
 
 namespace pdfp {
@@ -44,6 +45,30 @@ template <class Op>
 void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream) {
     if (s.n_tiles <= 0 || grid <= 0) return;
     tile_spmv_kernel<Op><<<grid, 2 * Op::NT + 32, tile_dyn_smem<Op>(s), stream>>>(s, op);
+}
+
+// ---- launching the flat engine ---------------------------------------------------
+
+template <class Op, int QPT>
+int flat_grid(const SideDev& s, int num_sms) {
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, flat_spmv_kernel<Op, QPT>, kFlatThreads, 0);
+    const int g = (blocks > 0 ? blocks : 1) * num_sms;
+    return g < s.n_tiles ? g : s.n_tiles;
+}
+
+template <class Op>
+int flat_grid(const SideDev& s, int qpt, int num_sms) {
+    return qpt == 1 ? flat_grid<Op, 1>(s, num_sms) : flat_grid<Op, 2>(s, num_sms);
+}
+
+template <class Op>
+void launch_flat(const SideDev& s, const Op& op, int qpt, int grid, cudaStream_t stream) {
+    if (s.n_tiles <= 0 || grid <= 0) return;
+    if (qpt == 1)
+        flat_spmv_kernel<Op, 1><<<grid, kFlatThreads, 0, stream>>>(s, op);
+    else
+        flat_spmv_kernel<Op, 2><<<grid, kFlatThreads, 0, stream>>>(s, op);
 }
 
 // ---- per-tile elementwise reductions and per-instance finalisation ---------------

@@ -124,6 +124,32 @@ struct HostTiling {
 void build_tiling(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
                   const StageGeom& g, HostTiling& t);
 
+// Caps of the flat step engine (flat_spmv.cuh): a multi-row tile holds at most
+// kFlatMaxRows rows and its nonzeros, counted from the 4-aligned element below
+// the first, at most `cap` (1024 or kFlatCapMax, the engine's two variants).
+constexpr int kFlatCapMax = 2048;
+constexpr int kFlatMaxRows = 256;
+
+// Stage size handed to the tiler for the flat engine: with at least one
+// 128-byte block for the row pointers, the 16-byte window of the column
+// indices can take at most 4 * cap bytes, the values' window correspondingly
+// (checked on every tiling by flat_tiling_fits).
+inline int32_t flat_stage_bytes(int esize_v, int cap) {
+    return static_cast<int32_t>(128u + 4u * cap + align128(static_cast<uint32_t>(esize_v) * cap));
+}
+
+inline bool flat_tiling_fits(const HostTiling& t, int cap) {
+    const size_t nt = t.tile_inst.size();
+    for (size_t i = 0; i < nt; ++i) {
+        const int32_t c = t.tile_chunk[i];
+        if (t.chunk_flags[c] & CHUNK_LONG) continue;
+        if (t.tile_chunk[i + 1] != c + 1 || t.tile_row[i + 1] - t.tile_row[i] > kFlatMaxRows ||
+            t.chunk_k1[c] - (t.chunk_k0[c] & ~3) > cap)
+            return false;
+    }
+    return true;
+}
+
 // One problem as handed to the library (CSR, caller's numbering).
 struct ProblemIn {
     int32_t m, n;

@@ -456,8 +456,23 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     // The autotuner pays for itself only where a step kernel takes longer than its
     // launch: below 256K nonzeros every candidate times the same few microseconds.
     // PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size.
+    // PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the step engine (flat1: one quad
+    // per thread and tile) and skips the tuner.
     const char* at = std::getenv("PDFP_AUTOTUNE");
-    const bool tune = at && at[0] == '0' ? false : (at && at[0] == '1' ? true : M_.L.NNZ >= (1 << 18));
+    const char* se = std::getenv("PDFP_STEP_ENGINE");
+    const int forced = !se ? -1
+                       : std::strcmp(se, "tile") == 0 ? 0
+                       : std::strcmp(se, "flat") == 0 || std::strcmp(se, "flat1") == 0 ? 1 : -1;
+    if (forced >= 0) {
+        const int qpt = std::strcmp(se, "flat1") == 0 ? 1 : 2;
+        for (StepSide* q : {&p32_, &d32_, &p64_, &d64_}) {
+            q->engine = forced;
+            q->qpt = qpt;
+        }
+    }
+    const bool tune = forced >= 0 ? false
+                      : at && at[0] == '0' ? false
+                      : (at && at[0] == '1' ? true : M_.L.NNZ >= (1 << 18));
     if (precision_ == PDFP_MIXED) {
         if (tune) autotune(true); else { prepare_side(p32_, true, true); prepare_side(d32_, false, true); }
     }
@@ -477,7 +492,9 @@ IterVecs<double>& Projector::vecs<double>() { return v64_; }
 template <typename T, bool MAJOR>
 void Projector::launch_primal(const StepSide& s, int k) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    if (s.nt == 256)
+    if (s.engine == 1)
+        launch_flat(s.tiling.dev, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
+    else if (s.nt == 256)
         launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_);
     else
         launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_);
@@ -486,7 +503,9 @@ void Projector::launch_primal(const StepSide& s, int k) {
 template <typename T, bool MAJOR>
 void Projector::launch_dual(const StepSide& s, int k) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    if (s.nt == 256)
+    if (s.engine == 1)
+        launch_flat(s.tiling.dev, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
+    else if (s.nt == 256)
         launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_);
     else
         launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_);
@@ -506,6 +525,22 @@ static int step_grid(const SideDev& d, int nt, int sms) {
 
 void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     const int e = f32 ? 4 : 8;
+    if (s.engine == 1) {
+        const int cap = s.qpt * 4 * kFlatThreads;
+        s.stage_bytes = flat_stage_bytes(e, cap);
+        s.nt = 0;
+        StageGeom g{e, e, e, 0, 1, s.stage_bytes, kFlatMaxRows};
+        s.tiling = M_.make_tiling(ar_, primal, g);
+        if (!flat_tiling_fits(s.tiling.host, cap))
+            throw Error(E_INVALID, "internal: a flat-engine tile exceeds the kernel's caps");
+        if (primal)
+            s.grid = f32 ? flat_grid<PrimalOp<float, false, kFlatThreads>>(s.tiling.dev, s.qpt, num_sms_)
+                         : flat_grid<PrimalOp<double, false, kFlatThreads>>(s.tiling.dev, s.qpt, num_sms_);
+        else
+            s.grid = f32 ? flat_grid<DualOp<float, false, kFlatThreads>>(s.tiling.dev, s.qpt, num_sms_)
+                         : flat_grid<DualOp<double, false, kFlatThreads>>(s.tiling.dev, s.qpt, num_sms_);
+        return;
+    }
     StageGeom g{e, e, e, primal ? 8 : 3, 1, s.stage_bytes, 2048};
     s.tiling = M_.make_tiling(ar_, primal, g);
     if (primal)
@@ -522,13 +557,15 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
 // all-zero state, which it resets afterwards.
 void Projector::autotune(bool f32) {
     struct Cand {
-        int stage, nt, l2;
+        int engine, stage, nt, l2, qpt;
     };
-    // 4 stages per block: 12-16 KB stages give 3-4 blocks per SM, 24 KB two, 32-48 KB one
+    // tile engine, 4 stages per block: 12-16 KB stages give 3-4 blocks per SM, 24 KB
+    // two, 32-48 KB one; then the flat engine with both gather cache policies
     static const Cand cands[] = {
-        {12 * 1024, 128, 0}, {16 * 1024, 128, 0}, {16 * 1024, 256, 0}, {24 * 1024, 256, 0},
-        {32 * 1024, 256, 0}, {48 * 1024, 256, 0}, {16 * 1024, 256, 1}, {24 * 1024, 256, 1},
-        {32 * 1024, 256, 1}};
+        {0, 12 * 1024, 128, 0, 0}, {0, 16 * 1024, 128, 0, 0}, {0, 16 * 1024, 256, 0, 0},
+        {0, 24 * 1024, 256, 0, 0}, {0, 32 * 1024, 256, 0, 0}, {0, 48 * 1024, 256, 0, 0},
+        {0, 16 * 1024, 256, 1, 0}, {0, 24 * 1024, 256, 1, 0}, {0, 32 * 1024, 256, 1, 0},
+        {1, 0, 0, 0, 2},           {1, 0, 0, 0, 1},           {1, 0, 0, 1, 2}};
     constexpr int NC = sizeof(cands) / sizeof(cands[0]);
     cudaEvent_t e0, e1;
     PDFP_CK(cudaEventCreate(&e0));
@@ -540,6 +577,8 @@ void Projector::autotune(bool f32) {
         std::vector<float> best_ms(NC, 1e30f);
         bool empty_side = false;
         for (int i = 0; i < NC; ++i) {
+            sides[i].engine = cands[i].engine;
+            if (cands[i].engine == 1) sides[i].qpt = cands[i].qpt;
             sides[i].stage_bytes = cands[i].stage;
             sides[i].nt = cands[i].nt;
             sides[i].gather_l2 = cands[i].l2;
@@ -577,7 +616,7 @@ void Projector::autotune(bool f32) {
         }
         int bi = 0;
         for (int i = 0; i < NC; ++i) {
-            tune_table_.push_back(TuneRow{side, cands[i].stage, cands[i].nt, cands[i].l2, best_ms[i]});
+            tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, best_ms[i]});
             if (best_ms[i] < best_ms[bi]) bi = i;
         }
         dst = sides[bi];

@@ -58,6 +58,8 @@ class Projector {
   private:
     // One side of the PDHG step: its tile geometry, block size and tiling.
     struct StepSide {
+        int engine = 0;  // 0: tile engine (tile_spmv.cuh), 1: flat engine (flat_spmv.cuh)
+        int qpt = 2;     // flat engine: quads (4 nonzeros) per thread and tile, 1 or 2
         int stage_bytes = 32 * 1024;
         int nt = 256;
         DeviceMatrix::Tiling tiling;
@@ -66,7 +68,7 @@ class Projector {
         float tuned_ms = 0.f;
     };
     struct TuneRow {
-        int side, stage, nt, l2;
+        int side, stage, nt, l2;  // nt = 0: the flat engine
         float ms;
     };
     std::vector<TuneRow> tune_table_;

@@ -11,9 +11,10 @@
 using namespace pdfp;
 
 static int check_tiling(const HostCsr& csr, const std::vector<int32_t>& off, const StageGeom& g,
-                        int64_t* n_tiles, int64_t* n_long) {
+                        int64_t* n_tiles, int64_t* n_long, int flat_cap = 0) {
     HostTiling t;
     build_tiling(csr, off, g, t);
+    if (flat_cap && !flat_tiling_fits(t, flat_cap)) return 26;
     const int K = static_cast<int>(off.size()) - 1;
     if (t.tile_row.size() != t.tile_inst.size() + 1) return 10;
     if ((int)t.inst_tile0.size() != K + 1) return 11;
@@ -108,5 +109,14 @@ extern "C" int layout_check(int K, const int32_t* ms, const int32_t* ns, const i
         rc = check_tiling(L.A, L.row_off, g, &stats[0], &stats[1]);
         if (rc) return 100 + rc;
     }
+    // the flat engine's geometries (FP32 and FP64 values, no staged vectors)
+    for (int e : {4, 8})
+        for (int cap : {1024, kFlatCapMax}) {
+            const StageGeom g{e, e, e, 0, 1, flat_stage_bytes(e, cap), kFlatMaxRows};
+            int rc = check_tiling(L.At, L.col_off, g, &stats[0], &stats[1], cap);
+            if (rc) return 200 + rc;
+            rc = check_tiling(L.A, L.row_off, g, &stats[0], &stats[1], cap);
+            if (rc) return 300 + rc;
+        }
     return 0;
 }

@@ -78,3 +78,12 @@ def test_null_arguments_are_rejected_without_touching_the_device():
     assert b"null" in L.lib().pdfp_last_error()
     assert L.lib().pdfp_set_target(None, 0, None) == L.E_INVALID
     assert L.lib().pdfp_solve(None, None, 1.0, None) == L.E_INVALID
+    assert L.lib().pdfp_measure_gather_rate(1024, 100, 1, None) == L.E_INVALID
+
+
+@pytest.mark.gpu
+def test_gather_rate_probe_reports_a_plausible_rate():
+    r = C.c_double()
+    L.check(L.lib().pdfp_measure_gather_rate(4_000_000, 1_000_000, 3, C.byref(r)))
+    assert 1e10 < r.value < 1e13  # gathers per second
+    assert L.lib().pdfp_measure_gather_rate(1023, 100, 1, C.byref(r)) == L.E_INVALID
