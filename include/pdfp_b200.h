@@ -187,7 +187,10 @@ PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
  * keeps the fastest per side; below 256K nonzeros it keeps the default.
  * PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size, and
  * PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the engine with its default
- * settings (flat1: the flat engine's one-quad-per-thread variant).
+ * settings (flat1: the flat engine's one-quad-per-thread variant), and
+ * PDFP_TUNING="s,t,l,s,t,l" pins both sides for handles created while it is
+ * set: stage bytes, threads per role and the L2-only flag of A', then of A,
+ * with the values out[] below reports.
  * out[8] = {A' stage bytes, A' threads per role (0: flat engine), A' tiles,
  * A stage bytes, A threads per role (0: flat engine), A tiles,
  * A' gathers L2-only, A gathers L2-only}. */

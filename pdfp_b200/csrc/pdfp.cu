@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <type_traits>
 #include <map>
@@ -30,6 +31,7 @@ namespace pdfp {
 constexpr int NT_EVAL = 256;
 constexpr int STALL_EVALS = 10;  // evaluations without 10% KKT progress before the FP64 polish
 constexpr double kFp32TolFloor = 1e-6;  // tighter relative tolerances run in FP64 from the start
+constexpr int64_t kMixedMinNnz = 1 << 18;  // smaller mixed handles compute in FP64
 
 // ---- per-instance state kernels ---------------------------------------------------
 
@@ -345,6 +347,14 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     if (!msg.empty()) throw Error(E_INVALID, msg);
     const HostLayout& L = M_.L;
     K_ = L.K;
+    // FP32 iterates pay only where the step kernels move enough bytes to be
+    // memory-bound; below kMixedMinNnz nonzeros (PDFP_MIXED_MIN_NNZ overrides)
+    // every launch is latency-bound and a mixed handle computes in FP64.
+    if (precision_ == PDFP_MIXED) {
+        const char* mm = std::getenv("PDFP_MIXED_MIN_NNZ");
+        const int64_t min_nnz = mm ? std::atoll(mm) : kMixedMinNnz;
+        if (L.NNZ < min_nnz) precision_ = PDFP_FP64;
+    }
     M_.upload(ar_, precision_ == PDFP_MIXED);
 
     // tilings of the evaluation passes (the step kernels' tilings are tuned below)
@@ -470,7 +480,34 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
             q->qpt = qpt;
         }
     }
-    const bool tune = forced >= 0 ? false
+    // PDFP_TUNING="s,t,l,s,t,l" pins both sides' step kernels of this precision
+    // (A' then A: stage bytes, threads per role -- 0: flat engine, whose stage
+    // bytes tell its variant -- and the L2-only gather flag), as pdfp_get_tuning
+    // reports them; the tuner does not run.
+    bool pinned = false;
+    if (const char* pt = std::getenv("PDFP_TUNING")) {
+        int v[6];
+        if (std::sscanf(pt, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) != 6)
+            throw Error(E_INVALID, "PDFP_TUNING must read stage,threads,l2,stage,threads,l2");
+        StepSide* sides[2][2] = {{&p32_, &d32_}, {&p64_, &d64_}};
+        for (int k = 0; k < 2; ++k)
+            for (int f = 0; f < 2; ++f) {
+                StepSide& q = *sides[f][k];
+                const int* c = v + 3 * k;
+                if (c[1] != 0 && c[1] != 128 && c[1] != 256)
+                    throw Error(E_INVALID, "PDFP_TUNING: threads per role must be 0, 128 or 256");
+                if (c[1] != 0 && (c[0] < 8192 || c[0] > 49152 || c[0] % 128 != 0))
+                    throw Error(E_INVALID, "PDFP_TUNING: tile-engine stage bytes must be a multiple "
+                                           "of 128 in [8192, 49152]");
+                q.engine = c[1] == 0 ? 1 : 0;
+                q.qpt = c[0] == 0 || c[0] == flat_stage_bytes(4, 1024) || c[0] == flat_stage_bytes(8, 1024) ? 1 : 2;
+                q.stage_bytes = c[0] > 0 ? c[0] : q.stage_bytes;
+                q.nt = c[1] == 0 ? 256 : c[1];
+                q.gather_l2 = c[2] != 0;
+            }
+        pinned = true;
+    }
+    const bool tune = forced >= 0 || pinned ? false
                       : at && at[0] == '0' ? false
                       : (at && at[0] == '1' ? true : M_.L.NNZ >= (1 << 18));
     if (precision_ == PDFP_MIXED) {

@@ -11,6 +11,11 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+# Mixed-precision handles below 2^18 nonzeros compute in FP64 by default; the
+# tests run the FP32 kernels on the small example models too (the threshold
+# itself is tested in test_gpu_flat.py).
+os.environ.setdefault("PDFP_MIXED_MIN_NNZ", "0")
 EXAMPLES = ["p0201", "pk1", "gen-ip054", "markshare2"]
 
 

@@ -54,3 +54,41 @@ def test_flat_and_tile_agree_mixed_with_long_rows(oracle, monkeypatch):
         assert res["tile"][0] == res[eng][0] == "OPTIMAL"
         assert abs(res["tile"][1] - res[eng][1]) <= 0.05 * res["tile"][1] + 64
         assert res[eng][2] == pytest.approx(res["tile"][2], rel=1e-3)
+
+
+def test_tuning_pin_and_bad_pin(oracle, examples, monkeypatch):
+    m = examples["pk1"]
+    xt = np.round(np.random.default_rng(2).random(len(m.c)))
+    monkeypatch.delenv("PDFP_STEP_ENGINE", raising=False)
+    monkeypatch.setenv("PDFP_TUNING", "12288,128,0,0,0,1")
+    sc, is_eq, is_int, w = oracle.projector_inputs(m)
+    s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+    tun = (gpu.C.c_int32 * 8)()
+    gpu.L.check(gpu.L.lib().pdfp_get_tuning(s._h, tun))
+    assert (tun[0], tun[1], tun[4], tun[6], tun[7]) == (12288, 128, 0, 0, 1)
+    s.set_target(xt / sc.D_c)
+    assert s.solve(SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-4), 1.0) == "OPTIMAL"
+    monkeypatch.setenv("PDFP_TUNING", "100,128,0,0,0,1")
+    with pytest.raises(Exception, match="stage bytes"):
+        gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+
+
+def test_small_mixed_handles_compute_in_fp64(oracle, examples, monkeypatch):
+    """Below 2^18 nonzeros a mixed handle is an FP64 handle (same steps, same
+    answer); PDFP_MIXED_MIN_NNZ=0 keeps FP32."""
+    m = examples["p0201"]
+    xt = np.round(np.random.default_rng(6).random(len(m.c)))
+    sc, is_eq, is_int, w = oracle.projector_inputs(m)
+    prm = SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-4)
+    out = {}
+    for label, prec, env in [("fp64", "fp64", None), ("auto", "mixed", None), ("fp32", "mixed", "0")]:
+        if env is None:
+            monkeypatch.delenv("PDFP_MIXED_MIN_NNZ", raising=False)
+        else:
+            monkeypatch.setenv("PDFP_MIXED_MIN_NNZ", env)
+        s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision=prec)
+        s.set_target(xt / sc.D_c)
+        s.solve(prm, 1.0)
+        out[label] = (s.last["precision"], s.total_count, s.pdhg_x)
+    assert out["auto"][0] == gpu.L.FP64 and out["fp32"][0] == gpu.L.MIXED
+    assert out["auto"][1] == out["fp64"][1] and np.array_equal(out["auto"][2], out["fp64"][2])
