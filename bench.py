@@ -332,8 +332,12 @@ def main():
     roof = None
     if mx["kp_ms"]:
         achieved = bytes_primal32 / (mx["kp_ms"] * 1e-3) / 1e9
+        # DRAM bytes of one launch of this kernel on the default workload, from one
+        # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
+        default = (args.workload, args.m, args.n, args.nnz) == ("zipf-lp", 1_000_000, 2_000_000,
+                                                                20_000_000)
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
+                "frac": round(achieved / peak, 4), "traffic": 253.1e6 if default else None,
                 "kernel": f"tile_spmv_kernel<PrimalOp<float, false, {mx['tuning']['a_t_threads']}>> (A'z + fused primal/y update)",
                 "peak_kind": peak_kind, "bytes_per_launch": bytes_primal32,
                 "mean_launch_ms": round(mx["kp_ms"], 5),
