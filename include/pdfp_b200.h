@@ -220,6 +220,20 @@ PDFP_API int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double
                        double* con_ub_out, double* D_r, double* D_c, double* bound_scale,
                        double* objective_scale);
 
+/* max_violation(milp, x), src/milp.jl:102-114, on the device: the largest
+ * violation of A x <= b (rows with is_eq[i] == 0) and A x = b (is_eq[i] != 0)
+ * over the ORIGINAL constraints (caller's numbering, 0-based CSR, ascending
+ * column indices), 0 when nothing is violated.  Rows are summed in ascending
+ * column order with separately rounded operations, so the value equals the
+ * host's A * x evaluation bit for bit.  A checker owns device copies of A, b
+ * and is_eq; pdfp_checker_max_violation copies x (n values) to the device and
+ * returns when the value is on the host.  Not re-entrant. */
+typedef struct pdfp_checker pdfp_checker;
+PDFP_API int pdfp_checker_create(const pdfp_csr* A, const double* b, const uint8_t* is_eq,
+                                 pdfp_checker** out);
+PDFP_API int pdfp_checker_max_violation(pdfp_checker* c, const double* x, double* violation);
+PDFP_API int pdfp_checker_destroy(pdfp_checker* c);
+
 /* Measurement support (no counterpart in the reference): the rate, in gathers
  * per second, at which this GPU serves `nnz` independent random 4-byte loads
  * from an m-entry FP32 vector when indices and values stream in coalesced --

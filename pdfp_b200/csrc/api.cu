@@ -245,6 +245,28 @@ int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double* var_lb,
     });
 }
 
+int pdfp_checker_create(const pdfp_csr* A, const double* b, const uint8_t* is_eq,
+                        pdfp_checker** out) {
+    return guarded([&] {
+        if (!A || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        *out = nullptr;
+        require_device();
+        *out = reinterpret_cast<pdfp_checker*>(pdfp::checker_create(*A, b, is_eq));
+    });
+}
+
+int pdfp_checker_max_violation(pdfp_checker* c, const double* x, double* violation) {
+    return guarded([&] {
+        if (!c || !violation) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        *violation = pdfp::checker_max_violation(*reinterpret_cast<pdfp::Checker*>(c), x);
+    });
+}
+
+int pdfp_checker_destroy(pdfp_checker* c) {
+    pdfp::checker_destroy(reinterpret_cast<pdfp::Checker*>(c));
+    return PDFP_OK;
+}
+
 int pdfp_measure_gather_rate(int64_t nnz, int32_t m, int32_t repeats, double* gathers_per_s) {
     return guarded([&] {
         if (!gathers_per_s) throw pdfp::Error(PDFP_E_INVALID, "null output");

@@ -25,4 +25,10 @@ void solve_lp_relaxation_device(const pdfp_csr& A, const double* c, const double
 // Random-gather ceiling of the current GPU (gatherprobe.cu): gathers per second.
 double measure_gather_rate(int64_t nnz, int32_t m, int32_t repeats);
 
+// The pump's constraint check on the device (checker.cu).
+struct Checker;
+Checker* checker_create(const pdfp_csr& A, const double* b, const uint8_t* is_eq);
+double checker_max_violation(Checker& c, const double* x);
+void checker_destroy(Checker* c);
+
 }  // namespace pdfp

@@ -196,6 +196,38 @@ class PDFPBatch:
         return out[:size]
 
 
+class ConstraintChecker:
+    """max_violation(milp, x) (src/milp.jl:102-114) on the device, bit-identical to
+    the host evaluation; keeps the original constraints on the GPU."""
+
+    def __init__(self, milp):
+        csr, keep = L.make_csr(milp.A)
+        self._keep = (keep, L.f64(milp.b), np.ascontiguousarray(milp.is_eq, dtype=np.uint8))
+        self.n = csr.n
+        self._h = C.c_void_p()
+        L.check(L.lib().pdfp_checker_create(C.byref(csr), L.dptr(self._keep[1]),
+                                            L.uptr(self._keep[2]), C.byref(self._h)))
+
+    def max_violation(self, x) -> float:
+        v = C.c_double()
+        xa = L.f64(x)
+        if len(xa) != self.n:
+            raise ValueError("x has the wrong length")
+        L.check(L.lib().pdfp_checker_max_violation(self._h, L.dptr(xa), C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.lib().pdfp_checker_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
 @dataclass
 class ScaledProblem:
     """src/preconditioner.jl:13-24"""

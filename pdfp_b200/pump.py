@@ -182,6 +182,15 @@ def _perturb(xt, x, milp: MILP, rng, general, is_general, ladder: RestartLadder,
             xt[j] = v
 
 
+def _violation_fn(milp: MILP, solvers):
+    """max_violation(milp, .) for the pump loop: on the device (bit-identical) when the
+    solvers offer it and the matrix is large enough for the copy of x to pay."""
+    if milp.A.nnz >= (1 << 16) and hasattr(solvers, "ConstraintChecker"):
+        checker = solvers.ConstraintChecker(milp)
+        return checker.max_violation
+    return lambda x: max_violation(milp, x)
+
+
 def _log(s: str) -> None:
     sys.stdout.write(s)
 
@@ -261,6 +270,7 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
                       swap_iteration=swap_iteration,
                       policy=BatchPolicy() if batch_policy == "cost" else None)
     stats = PumpCounters()
+    viol = _violation_fn(milp, solvers)
     if verbose:
         _print_header(milp, solvers.device_name())
 
@@ -321,7 +331,7 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
         _log("%6s %12s %10s %10s %9s %8s %9s\n" % (
             "iter", "distance", "violation", "pdhg", "gap tol", "action", "time"))
     while elapsed() < time_limit:
-        violation = max_violation(milp, xt)
+        violation = viol(xt)
         if violation <= tol and is_integral(xt, int_idx, tol):
             return _finish(milp, True, xt.copy(), stats, elapsed(), verbose)
         stats.iterations += 1
@@ -341,7 +351,7 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
         inner = projector.total_count
         while (mixed and tightening_budget > 1e-6 and elapsed() < time_limit
                and is_integral(x, int_idx, tol)
-               and max_violation(milp, _round_to_nearest(x, milp)) > tol):
+               and viol(_round_to_nearest(x, milp)) > tol):
             tightening_budget *= 0.1
             gap = max(gap * 0.1, 1e-8)
             params = SolverParameters(iteration_limit=projection_iteration_limit,
@@ -360,7 +370,7 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
 
         if is_integral(x, int_idx, tol):
             candidate = _round_to_nearest(x, milp)
-            if max_violation(milp, candidate) <= tol:
+            if viol(candidate) <= tol:
                 if verbose:
                     _print_iteration(iteration, distance, violation, inner, gap_used, "integral",
                                      elapsed())
@@ -492,6 +502,7 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
     tol = feasibility_tolerance
     mixed = num_continuous(milp) > 0
     stats = PumpCounters()
+    viol = _violation_fn(milp, solvers)
     x, dual_slack, stats.root_lp_status, _ = solvers.solve_lp_relaxation(
         milp, tolerance=root_lp_tolerance, time_limit=remaining(), cupdlpx_termination=mixed)
     stats.root_lp_time = elapsed()
@@ -532,7 +543,7 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
         if (stop(done) if stop is not None else done):
             break
         for p, tr in enumerate(trajs):
-            if max_violation(milp, tr.xt) <= tol and is_integral(tr.xt, int_idx, tol):
+            if viol(tr.xt) <= tol and is_integral(tr.xt, int_idx, tol):
                 tr.found, tr.x_found, tr.t_found = True, tr.xt.copy(), elapsed()
                 winner = p
                 break
@@ -549,7 +560,7 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
         # mixed models: tenfold tighter re-solves (src/pump.jl:343-356), batched
         while mixed and elapsed() < time_limit:
             need = [p for p in range(K) if budgets[p] > 1e-6 and is_integral(xs[p], int_idx, tol)
-                    and max_violation(milp, _round_to_nearest(xs[p], milp)) > tol]
+                    and viol(_round_to_nearest(xs[p], milp)) > tol]
             if not need:
                 break
             for p in need:
@@ -568,7 +579,7 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
             xp = xs[p]
             if is_integral(xp, int_idx, tol):
                 cand = _round_to_nearest(xp, milp)
-                if max_violation(milp, cand) <= tol:
+                if viol(cand) <= tol:
                     tr.found, tr.x_found, tr.t_found = True, cand, elapsed()
                     winner = p
                     break
