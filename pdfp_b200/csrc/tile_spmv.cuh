@@ -13,10 +13,13 @@
 //             and -- on a tile's last chunk -- the slices of the per-row vectors
 //             the epilogue reads, completing on the stage's FULL mbarrier; it
 //             waits on the stage's EMPTY mbarrier before reusing it.
-//   GATHERERS (NT threads) wait on FULL and compute the products
-//             p_k = a_k * g[col_k] of every nonzero, thread-strided with eight
+//   GATHERERS (NT threads) each wait on FULL and compute their share of the
+//             products p_k = a_k * g[col_k], thread-strided with up to sixteen
 //             gathers in flight per thread (the gathered vector is L2-resident),
-//             in place over the staged values; then arrive on PROD.
+//             in place over the staged values; then each arrives on PROD (which
+//             completes when all NT have).  No barrier joins them, so threads
+//             drift up to kStages stages apart and gathers of several stages
+//             overlap.
 //   REDUCERS  (NT threads) wait on PROD, sum each row in shared memory (G lanes
 //             per row; G = 1 sums a row sequentially in ascending storage order,
 //             which is the reference's order; a long row uses a block
@@ -26,7 +29,7 @@
 //             term) of the Op; then arrive on EMPTY.
 //
 // So the gathers of one chunk are in flight while the rows of the previous one
-// are reduced and updated.  Each role synchronises internally with its own
+// are reduced and updated.  The reducers synchronise among themselves with a
 // named barrier; every wait is bounded.
 //
 // The Op supplies the types, the gathered vectors, the staged vectors and the
@@ -39,7 +42,6 @@
 namespace pdfp {
 
 constexpr int kStages = 4;     // shared-memory stages per block
-constexpr int kGatherBar = 1;  // named barrier id of the gatherer threads
 constexpr int kReduceBar = 2;  // named barrier id of the reducer threads
 
 // Where each region of a chunk lives inside a stage buffer.
@@ -136,7 +138,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     if (threadIdx.x == 0) {
         for (int i = 0; i < kStages; ++i) {
             mbar_init(&sh.full[i], 1);
-            mbar_init(&sh.prod[i], 1);
+            mbar_init(&sh.prod[i], Op::NT);  // every gatherer arrives
             mbar_init(&sh.empty[i], 1);
         }
         sh.flag = 0;
@@ -174,8 +176,11 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         const int g = threadIdx.x;
         for (uint32_t u = 0;; ++u) {
             const int st = u % kStages;
-            const bool ok = group_wait(&sh.full[st], (u / kStages) & 1u, op.err(), g == 0,
-                                       kGatherBar, NT, &sh.flag);
+            // Each gatherer waits and arrives on its own: with no barrier among them a
+            // thread whose gathers have landed runs ahead into the next stages while
+            // slower gathers of the previous one are still in flight.
+            const bool ok = mbar_wait_bounded(&sh.full[st], (u / kStages) & 1u, op.err());
+            if (!ok) sh.flag = 1;
             const int32_t c = ok ? sh.stage_chunk[st] : -1;
             if (c >= 0 && NV > 0) {
                 unsigned char* buf = dyn_smem + st * (size_t)s.stage_bytes;
@@ -256,9 +261,8 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                         }
                     }
                 }
-                named_sync(kGatherBar, NT);
             }
-            if (g == 0) mbar_arrive(&sh.prod[st]);  // products of this stage are in place
+            mbar_arrive(&sh.prod[st]);  // this thread's products of the stage are in place
             if (c < 0) break;
         }
         return;
