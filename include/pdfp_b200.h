@@ -220,6 +220,23 @@ PDFP_API int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double
                        double* con_ub_out, double* D_r, double* D_c, double* bound_scale,
                        double* objective_scale);
 
+/* read_mps (src/milp.jl:42-94) on the host, in C++: an MPS file, plain or
+ * gzip-compressed (zlib), into the pump's canonical form -- min c'x + c0 s.t.
+ * A x <= b (is_eq[i] == 0) / A x = b (is_eq[i] != 0), l <= x <= u, x_j integer
+ * for j in int_idx -- with the reference's canonicalisation (maximisation
+ * negated, binaries clipped to [0, 1], equal finite row bounds -> equality,
+ * else hi row then -lo row, |v| >= 1e20 infinite).  CSR rows list their
+ * columns ascending (0-based).  pdfp_mps_dims gives the sizes, pdfp_mps_get
+ * copies the arrays out (c, l, u: n; b, is_eq: m; row_ptr: m + 1; col_idx,
+ * val: nnz; int_idx: n_int).  Needs no GPU. */
+typedef struct pdfp_mps pdfp_mps;
+PDFP_API int pdfp_mps_read(const char* path, pdfp_mps** out);
+PDFP_API int pdfp_mps_dims(const pdfp_mps* p, int32_t* m, int32_t* n, int64_t* nnz, int32_t* n_int);
+PDFP_API int pdfp_mps_get(const pdfp_mps* p, double* c, double* c0, int32_t* row_ptr,
+                          int32_t* col_idx, double* val, double* b, uint8_t* is_eq, double* l,
+                          double* u, int32_t* int_idx);
+PDFP_API int pdfp_mps_destroy(pdfp_mps* p);
+
 /* max_violation(milp, x), src/milp.jl:102-114, on the device: the largest
  * violation of A x <= b (rows with is_eq[i] == 0) and A x = b (is_eq[i] != 0)
  * over the ORIGINAL constraints (caller's numbering, 0-based CSR, ascending

@@ -110,6 +110,10 @@ SIGNATURES = {
                                      C.c_int32, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]),
     "pdfp_estimate_max_singular_value": (C.c_int, [C.POINTER(Csr), C.c_int32, C.c_double, dp, ip]),
     "pdfp_measure_gather_rate": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, dp]),
+    "pdfp_mps_read": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
+    "pdfp_mps_dims": (C.c_int, [vp, ip, ip, C.POINTER(C.c_int64), ip]),
+    "pdfp_mps_get": (C.c_int, [vp, dp, dp, ip, ip, dp, dp, up, dp, dp, ip]),
+    "pdfp_mps_destroy": (C.c_int, [vp]),
     "pdfp_checker_create": (C.c_int, [C.POINTER(Csr), dp, up, C.POINTER(vp)]),
     "pdfp_checker_max_violation": (C.c_int, [vp, dp, dp]),
     "pdfp_checker_destroy": (C.c_int, [vp]),

@@ -10,6 +10,7 @@
 #include "../../include/pdfp_b200.h"
 #include "device.hpp"
 #include "projector.hpp"
+#include "mps.hpp"
 #include "solvers.hpp"
 
 namespace pdfp {
@@ -243,6 +244,53 @@ int pdfp_scale_problem(const pdfp_csr* A, const double* c, const double* var_lb,
                                    c_out, var_lb_out, var_ub_out, con_lb_out, con_ub_out, D_r, D_c,
                                    bound_scale, objective_scale);
     });
+}
+
+int pdfp_mps_read(const char* path, pdfp_mps** out) {
+    return guarded([&] {
+        if (!path || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        *out = nullptr;
+        *out = reinterpret_cast<pdfp_mps*>(pdfp::read_mps_file(path));
+    });
+}
+
+int pdfp_mps_dims(const pdfp_mps* p, int32_t* m, int32_t* n, int64_t* nnz, int32_t* n_int) {
+    return guarded([&] {
+        if (!p || !m || !n || !nnz || !n_int) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        const pdfp::MpsModel& M = *reinterpret_cast<const pdfp::MpsModel*>(p);
+        *m = M.m;
+        *n = M.n;
+        *nnz = static_cast<int64_t>(M.ci.size());
+        *n_int = static_cast<int32_t>(M.int_idx.size());
+    });
+}
+
+int pdfp_mps_get(const pdfp_mps* p, double* c, double* c0, int32_t* row_ptr, int32_t* col_idx,
+                 double* val, double* b, uint8_t* is_eq, double* l, double* u, int32_t* int_idx) {
+    return guarded([&] {
+        if (!p || !c0 || !row_ptr) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        const pdfp::MpsModel& M = *reinterpret_cast<const pdfp::MpsModel*>(p);
+        auto put = [](auto* dst, const auto& src) {
+            if (src.empty()) return;
+            if (!dst) throw pdfp::Error(PDFP_E_INVALID, "null output array");
+            std::memcpy(dst, src.data(), sizeof(src[0]) * src.size());
+        };
+        *c0 = M.c0;
+        put(c, M.c);
+        put(row_ptr, M.rp);
+        put(col_idx, M.ci);
+        put(val, M.v);
+        put(b, M.b);
+        put(is_eq, M.is_eq);
+        put(l, M.l);
+        put(u, M.u);
+        put(int_idx, M.int_idx);
+    });
+}
+
+int pdfp_mps_destroy(pdfp_mps* p) {
+    pdfp::mps_destroy(reinterpret_cast<pdfp::MpsModel*>(p));
+    return PDFP_OK;
 }
 
 int pdfp_checker_create(const pdfp_csr* A, const double* b, const uint8_t* is_eq,

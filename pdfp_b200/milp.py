@@ -302,6 +302,35 @@ def read_mps(path: str) -> MILP:
     return MILP(c, c0, A, np.array(b), sense, l, u, np.array(int_idx, dtype=np.int64), cols, name)
 
 
+def read_mps_native(path: str) -> MILP:
+    """``read_mps`` through the library's C++ reader (zlib for .gz; no GPU needed):
+    the same canonical model, built without the interpreter's per-line cost."""
+    import ctypes as C  # noqa: PLC0415
+
+    from . import _lib as L  # noqa: PLC0415
+    h = C.c_void_p()
+    L.check(L.lib().pdfp_mps_read(os.fsencode(path), C.byref(h)))
+    try:
+        m, n, n_int = C.c_int32(), C.c_int32(), C.c_int32()
+        nnz = C.c_int64()
+        L.check(L.lib().pdfp_mps_dims(h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(n_int)))
+        M, N, Z, NI = m.value, n.value, nnz.value, n_int.value
+        c, l, u = np.zeros(max(N, 1)), np.zeros(max(N, 1)), np.zeros(max(N, 1))
+        b, is_eq = np.zeros(max(M, 1)), np.zeros(max(M, 1), dtype=np.uint8)
+        rp = np.zeros(M + 1, dtype=np.int32)
+        ci, v = np.zeros(max(Z, 1), dtype=np.int32), np.zeros(max(Z, 1))
+        ii = np.zeros(max(NI, 1), dtype=np.int32)
+        c0 = C.c_double()
+        L.check(L.lib().pdfp_mps_get(h, L.dptr(c), C.byref(c0), L.iptr(rp), L.iptr(ci), L.dptr(v),
+                                     L.dptr(b), L.uptr(is_eq), L.dptr(l), L.dptr(u), L.iptr(ii)))
+    finally:
+        L.lib().pdfp_mps_destroy(h)
+    A = sp.csr_matrix((v[:Z], ci[:Z], rp), shape=(M, N))
+    name = re.sub(r"\.mps(\.gz)?$", "", os.path.basename(path))
+    return MILP(c[:N], c0.value, A, b[:M], ["eq" if e else "le" for e in is_eq[:M]], l[:N], u[:N],
+                ii[:NI].astype(np.int64), [], name)
+
+
 # ---------------------------------------------------------------------------
 # checks
 
