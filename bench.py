@@ -606,5 +606,17 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def shutdown():
+    try:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
+    except Exception:  # noqa: BLE001
+        pass
+
+
 if __name__ == "__main__":
-    main()
+    try:
+        main()
+    finally:
+        shutdown()
