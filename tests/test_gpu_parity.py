@@ -342,3 +342,29 @@ def test_empty_constraint_set(oracle):
     assert st == "OPTIMAL"
     x = s.pdhg_x
     assert x[0] == pytest.approx(0.5, abs=1e-6) and x[1] == pytest.approx(2.0, abs=1e-6)
+
+
+def test_uneven_batch_members_follow_the_oracle(oracle):
+    """Config-3 shape at test scale: 12 covering/packing models, n log-uniform in
+    [300, 6000], one FP64 batch handle; every member takes the oracle's steps."""
+    models = synthetic.covering_packing_batch(seed=5, k=12, n_min=300, n_max=6000)
+    probs, targets, scs = [], [], []
+    rng = np.random.default_rng(12)
+    for m in models:
+        sc, is_eq, is_int, w = proj_inputs(oracle, m)
+        probs.append((sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w))
+        targets.append(np.round(rng.random(len(m.c))))
+        scs.append(sc)
+    b = gpu.PDFPBatch(probs, precision="fp64")
+    for p, xt in enumerate(targets):
+        b.set_target(p, xt / scs[p].D_c)
+    prm = SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-5)
+    st = b.solve(prm, 1.0)
+    for p, m in enumerate(models):
+        sc, is_eq, is_int, w = proj_inputs(oracle, m)
+        twin = oracle.OracleSolvers.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb,
+                                               sc.var_ub, w)
+        twin.set_target(targets[p] / sc.D_c)
+        status = twin.solve(prm, 1.0)
+        assert st[p] == status and b.results[p]["total_count"] == twin.total_count, p
+        assert np.abs(b.get(p, "pdhg_x") - twin.pdhg_x).max() <= 1e-10, p
