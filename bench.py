@@ -391,7 +391,7 @@ def main():
     windows = mx["iters"] // 200
     line["gpu_launches"] = int(windows * (2 * 200 + 10) + args.steps * 12)
     line["clocks"] = mx["clocks"]
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the host baseline is measured at N = 1 only
         t = time.time()
         line["cpu_baseline"] = cpu_baseline(sc, w, xt0, is_eq, is_int, 1, args.cpu_iterations,
                                             "single thread")
