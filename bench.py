@@ -13,7 +13,8 @@ flipped.  `value` = PDHG iterations of the timed projections / their device
 time (CUDA events on the library's stream), mixed precision; the plain FP64
 form is measured on the same sequence of targets and reported beside it.
 With N > 1 every rank solves its own replica (a single projection does not
-shard) and `value` sums iterations over ranks / max time.
+shard: each iteration would need an all-gather of x_bar and z) and `value` sums
+iterations over ranks / max time.
 
 --impl reference times the reference's own CPU algorithm (the C restatement
 under oracle/, every host thread) on a bounded sample of the same workload:
@@ -27,6 +28,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -88,7 +90,7 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"pdfp_bench_clocks_{os.getpid()}_{gpu_index}.csv")
 
     def __enter__(self):
         try:
