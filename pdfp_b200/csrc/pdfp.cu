@@ -24,6 +24,7 @@
 #include "pdfp_ops.cuh"
 #include "controller.cuh"
 #include "power.cuh"
+#include "tiny_steps.cuh"
 #include "projector.hpp"
 
 namespace pdfp {
@@ -32,6 +33,8 @@ constexpr int NT_EVAL = 256;
 constexpr int STALL_EVALS = 10;  // evaluations without 10% KKT progress before the FP64 polish
 constexpr double kFp32TolFloor = 1e-6;  // tighter relative tolerances run in FP64 from the start
 constexpr int64_t kMixedMinNnz = 1 << 18;  // smaller mixed handles compute in FP64
+constexpr int64_t kTinyMaxDim = 4096;      // rows + columns of a member for the one-launch steps
+constexpr int64_t kTinyMaxNnz = 1 << 16;   // nonzeros of a member for the one-launch steps
 
 // ---- per-instance state kernels ---------------------------------------------------
 
@@ -356,6 +359,18 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
         if (L.NNZ < min_nnz) precision_ = PDFP_FP64;
     }
     M_.upload(ar_, precision_ == PDFP_MIXED);
+    // Small members (every one at most kTinyMaxDim rows + columns and
+    // kTinyMaxNnz nonzeros; PDFP_TINY=0 switches this off): the minor steps of a
+    // window run in one launch, one block per member.
+    {
+        const char* te = std::getenv("PDFP_TINY");
+        tiny_ = !(te && te[0] == '0') && K_ <= 65535;
+        for (int p = 0; p < K_ && tiny_; ++p) {
+            const int64_t dim = (L.row_off[p + 1] - L.row_off[p]) + (L.col_off[p + 1] - L.col_off[p]);
+            const int64_t nz = L.A.rp[L.row_off[p + 1]] - L.A.rp[L.row_off[p]];
+            if (dim > kTinyMaxDim || nz > kTinyMaxNnz) tiny_ = false;
+        }
+    }
 
     // tilings of the evaluation passes (the step kernels' tilings are tuned below)
     StageGeom gev{8, 8, 8, 0, 2, 32 * 1024, 2048};
@@ -803,6 +818,16 @@ void Projector::ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance
     PDFP_CK(cudaStreamSynchronize(stream_));
 }
 
+template <typename T>
+void Projector::launch_tiny_steps(int i0, int i1) {
+    const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    tiny_steps_kernel<T><<<K_, kTinyThreads, 0, stream_>>>(
+        PrimalOp<T, false, kTinyThreads>{vecs<T>(), st_, 0, mode, err_, 0},
+        DualOp<T, false, kTinyThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, 0, mode, err_, 0},
+        M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, i0, i1);
+    PDFP_CK(cudaGetLastError());
+}
+
 void Projector::record_window(int freq, bool with32, bool with64) {
     const int mode32 = MODE_FP32, mode64 = MODE_FP64;
     auto prim32 = [&](int k, bool major) {
@@ -830,6 +855,13 @@ void Projector::record_window(int freq, bool with32, bool with64) {
     const bool sample = timing_ && freq >= 3 && (with32 != with64);
     for (int i = 1; i <= freq; ++i) {
         const bool major = (i == 1 || i == freq);
+        if (tiny_ && !sample && i == 2 && freq > 2) {
+            // steps 2 .. freq-1 in one launch per precision
+            if (with32) launch_tiny_steps<float>(2, freq);
+            if (with64) launch_tiny_steps<double>(2, freq);
+            i = freq - 1;
+            continue;
+        }
         if (sample && i == 2) {
             // events around one minor step of each kernel (timing mode)
             PDFP_CK(cudaEventRecordWithFlags(tev_[0], stream_, cudaEventRecordExternal));

@@ -83,6 +83,8 @@ class Projector {
     void check_instance(int p) const;
     void ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance);
     void record_window(int freq, bool with32, bool with64);
+    template <typename T>
+    void launch_tiny_steps(int i0, int i1);
     cudaGraphExec_t window_graph(int freq, bool with32, bool with64);
 
     int precision_;
@@ -113,6 +115,7 @@ class Projector {
     } g_;
     std::map<int, cudaGraphExec_t> graphs_;
     bool timing_ = false;
+    bool tiny_ = false;  // every member small: a window's minor steps run in one launch
     cudaEvent_t tev_[3] = {nullptr, nullptr, nullptr};     // sampled step kernels (timing mode)
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
 };

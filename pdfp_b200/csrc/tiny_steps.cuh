@@ -1,0 +1,80 @@
+// tiny_steps.cuh -- the minor steps of a window in one launch, for small instances.
+//
+// For instances of a few thousand rows and columns every step launch is
+// latency-bound: two launches per PDHG step cost more than the step itself.
+// Here one block per batch member runs steps i0 .. i1-1 of an evaluation window
+// back to back, with a block barrier between the A'-side and the A-side pass
+// and after each step; vectors stay in global memory (L1/L2-resident at these
+// sizes).  Each pass sums a row with G lanes, lane-strided partial sums reduced
+// by an xor tree -- G = 1, a sequential sum in storage order (the reference's
+// order), whenever the side has more than half as many rows as the block has
+// threads -- and applies the Op's own per-row epilogue.  The first and last
+// (major) steps of a window, the evaluations and the controller run as before.
+#pragma once
+#include "common.cuh"
+#include "pdfp_ops.cuh"
+
+namespace pdfp {
+
+constexpr int kTinyThreads = 256;
+
+template <class Op>
+__device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restrict__ rp,
+                                          const int32_t* __restrict__ ci, int32_t r0, int32_t r1,
+                                          int inst) {
+    using AT = typename Op::AT;
+    using GT = typename Op::GT;
+    using VT = typename Op::VT;
+    constexpr int NVEC = Op::NVEC;
+    const VT* sv[NVEC];
+#pragma unroll
+    for (int k = 0; k < NVEC; ++k) sv[k] = op.staged(k);
+    const typename Op::TileP tp = op.tile_params(inst);
+    const auto* vals = op.values();
+    double none[1] = {0.0};
+    const int32_t R = r1 - r0;
+    int G = 1;
+    while (G < 32 && G * 2 * R <= kTinyThreads) G *= 2;
+    const int groups = kTinyThreads / G;
+    const int gid = threadIdx.x / G, lane = threadIdx.x & (G - 1);
+    for (int32_t b = 0; b < R; b += groups) {
+        const int32_t rr = b + gid;
+        AT s = AT(0);
+        if (rr < R) {
+            const int32_t row = r0 + rr;
+            for (int32_t k = rp[row] + lane; k < rp[row + 1]; k += G) {
+                GT g[1];
+                op.gather(ci[k], g);
+                s = add_rn(s, mul_rn(static_cast<AT>(vals[k]), static_cast<AT>(g[0])));
+            }
+        }
+        for (int o = G >> 1; o > 0; o >>= 1) s = add_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+        if (rr < R && lane == 0) {
+            const AT sums[1] = {s};
+            op.row(r0 + rr, r0 + rr, inst, tp, sv, sums, none);
+        }
+    }
+}
+
+// Steps i0 .. i1-1 (minor: no pdhg_* / reflected_* outputs) of instance blockIdx.x.
+template <typename T>
+__global__ void __launch_bounds__(kTinyThreads)
+    tiny_steps_kernel(PrimalOp<T, false, kTinyThreads> pop, DualOp<T, false, kTinyThreads> dop,
+                      const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
+                      const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
+                      const int32_t* __restrict__ col_off, const int32_t* __restrict__ row_off,
+                      int32_t i0, int32_t i1) {
+    const int p = blockIdx.x;
+    if (!pop.active(p)) return;  // block-uniform; status changes only in the controller
+    const int32_t c0 = col_off[p], c1 = col_off[p + 1], r0 = row_off[p], r1 = row_off[p + 1];
+    for (int32_t i = i0; i < i1; ++i) {
+        pop.k_offset = i;
+        dop.k_offset = i;
+        tiny_pass(pop, rp_t, ci_t, c0, c1, p);  // A'z, primal_step! and dual_y_step!
+        __syncthreads();
+        tiny_pass(dop, rp_a, ci_a, r0, r1, p);  // A x_bar and dual_z_step!
+        __syncthreads();
+    }
+}
+
+}  // namespace pdfp

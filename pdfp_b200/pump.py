@@ -182,10 +182,13 @@ def _perturb(xt, x, milp: MILP, rng, general, is_general, ladder: RestartLadder,
             xt[j] = v
 
 
+DEVICE_CHECK_MIN_NNZ = 1 << 16  # smaller matrices are checked on the host
+
+
 def _violation_fn(milp: MILP, solvers):
     """max_violation(milp, .) for the pump loop: on the device (bit-identical) when the
     solvers offer it and the matrix is large enough for the copy of x to pay."""
-    if milp.A.nnz >= (1 << 16) and hasattr(solvers, "ConstraintChecker"):
+    if milp.A.nnz >= DEVICE_CHECK_MIN_NNZ and hasattr(solvers, "ConstraintChecker"):
         checker = solvers.ConstraintChecker(milp)
         return checker.max_violation
     return lambda x: max_violation(milp, x)

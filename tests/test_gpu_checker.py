@@ -47,3 +47,19 @@ def test_checker_equals_host_large_with_empty_rows():
         assert ck.max_violation(x) == max_violation(m2, x)
     with pytest.raises(ValueError):
         ck.max_violation(np.zeros(3))
+
+
+@pytest.mark.gpu
+def test_pump_with_device_check_takes_the_same_steps(examples, monkeypatch):
+    """The pump's decisions do not depend on where max_violation runs."""
+    import pdfp_b200.pump as P
+    m = examples["pk1"]
+    runs = []
+    for threshold in (1 << 40, 0):  # host check, then device check
+        monkeypatch.setattr(P, "DEVICE_CHECK_MIN_NNZ", threshold)
+        r = P.feasibility_pump(m, time_limit=120.0, precision="fp64", seed=5, batch_policy="always")
+        runs.append(r)
+    a, b = runs
+    assert (a.found, a.iterations, a.perturbations, a.pdhg_iterations) == \
+        (b.found, b.iterations, b.perturbations, b.pdhg_iterations)
+    assert np.array_equal(a.x, b.x)

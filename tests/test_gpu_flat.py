@@ -92,3 +92,33 @@ def test_small_mixed_handles_compute_in_fp64(oracle, examples, monkeypatch):
         out[label] = (s.last["precision"], s.total_count, s.pdhg_x)
     assert out["auto"][0] == gpu.L.FP64 and out["fp32"][0] == gpu.L.MIXED
     assert out["auto"][1] == out["fp64"][1] and np.array_equal(out["auto"][2], out["fp64"][2])
+
+
+@pytest.mark.parametrize("name", ["p0201", "pk1", "markshare2"])
+def test_one_launch_minor_steps(oracle, examples, name, monkeypatch):
+    """Small members run a window's minor steps in one launch.  FP64: the oracle's
+    steps (status, iteration count, iterates within 1e-10); mixed: the two-launch
+    form's answer (same status, counts within 5%, l1 distance within 1e-6 relative)."""
+    m = examples[name]
+    xt = np.round(np.random.default_rng(8).random(len(m.c)) * (np.minimum(m.u, 2) - m.l) + m.l)
+    sc, is_eq, is_int, w = oracle.projector_inputs(m)
+    prm = SolverParameters(eps_optimal_relative=1e-6, eps_feasible_relative=1e-6)
+    monkeypatch.setenv("PDFP_TINY", "1")
+    s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="fp64")
+    s.set_target(xt / sc.D_c)
+    st = s.solve(prm, 1.0)
+    o = oracle.OracleSolvers.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w)
+    o.set_target(xt / sc.D_c)
+    assert st == o.solve(prm, 1.0) and s.total_count == o.total_count
+    assert np.abs(s.pdhg_x - o.pdhg_x).max() <= 1e-10
+    res = {}
+    for tiny in ("0", "1"):
+        monkeypatch.setenv("PDFP_TINY", tiny)
+        s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+        s.set_target(xt / sc.D_c)
+        st = s.solve(SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-4), 1.0)
+        I = m.int_idx
+        res[tiny] = (st, s.total_count, float(np.sum(w[I] * np.abs(s.pdhg_x[I] - xt[I] / sc.D_c[I]))))
+    assert res["0"][0] == res["1"][0]
+    assert abs(res["0"][1] - res["1"][1]) <= 0.05 * res["0"][1] + 200
+    assert res["1"][2] == pytest.approx(res["0"][2], rel=1e-6, abs=1e-9)
