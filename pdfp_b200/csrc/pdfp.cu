@@ -821,7 +821,8 @@ void Projector::ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance
 template <typename T>
 void Projector::launch_tiny_steps(int i0, int i1) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    tiny_steps_kernel<T><<<K_, kTinyThreads, 0, stream_>>>(
+    tiny_steps_kernel<PrimalOp<T, false, kTinyThreads>, DualOp<T, false, kTinyThreads>>
+        <<<K_, kTinyThreads, 0, stream_>>>(
         PrimalOp<T, false, kTinyThreads>{vecs<T>(), st_, 0, mode, err_, 0},
         DualOp<T, false, kTinyThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, 0, mode, err_, 0},
         M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, i0, i1);

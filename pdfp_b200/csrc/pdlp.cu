@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -17,6 +18,7 @@
 #include "device.hpp"
 #include "kernels.cuh"
 #include "pdlp_ops.cuh"
+#include "tiny_steps.cuh"
 #include "power.cuh"
 #include "solvers.hpp"
 
@@ -258,6 +260,11 @@ class LpSolver {
         std::string msg = build_layout({in}, false, M_.L);  // caller order: no permutation
         if (!msg.empty()) throw Error(E_INVALID, msg);
         M_.upload(ar_, f32_);
+        {
+            const char* te = std::getenv("PDFP_TINY");
+            tiny_ = !(te && te[0] == '0') && static_cast<int64_t>(A.m) + A.n <= 4096 &&
+                    M_.L.NNZ <= (1 << 16);
+        }
         m_ = A.m;
         n_ = A.n;
         const int e = f32_ ? 4 : 8;
@@ -367,6 +374,7 @@ class LpSolver {
     void prepare_grids();
 
     bool cupdlpx_, f32_;
+    bool tiny_ = false;  // small LP: a window's minor steps in one launch
     int sms_ = 148;
     int32_t m_ = 0, n_ = 0;
     cudaStream_t stream_ = nullptr;
@@ -433,7 +441,17 @@ void LpSolver::record(int freq) {
     evals(EVAL_AFTER_RESTART);
     launch_finalize(1, LpController{ev_t_.inst_tile0, d_.part_col, ev_a_.inst_tile0, d_.part_row,
                                     st_, flags_, 0, cupdlpx_ ? 1 : 0}, stream_);
-    for (int i = 2; i <= freq - 1; ++i) step(i, false);
+    if (tiny_ && freq > 2) {
+        // a small LP: steps 2 .. freq-1 in one launch (tiny_steps.cuh)
+        tiny_steps_kernel<LpPrimalOp<T, false, kTinyThreads>, LpDualOp<T, false, kTinyThreads>>
+            <<<1, kTinyThreads, 0, stream_>>>(LpPrimalOp<T, false, kTinyThreads>{v, st_, 0, mode, err_},
+                                              LpDualOp<T, false, kTinyThreads>{v, st_, 0, mode, err_},
+                                              M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off,
+                                              M_.row_off, 2, freq);
+        PDFP_CK(cudaGetLastError());
+    } else {
+        for (int i = 2; i <= freq - 1; ++i) step(i, false);
+    }
     step(freq, true);
     evals(EVAL_FULL);
     if (cupdlpx_) {

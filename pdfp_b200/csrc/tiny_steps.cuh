@@ -12,7 +12,6 @@
 // (major) steps of a window, the evaluations and the controller run as before.
 #pragma once
 #include "common.cuh"
-#include "pdfp_ops.cuh"
 
 namespace pdfp {
 
@@ -56,10 +55,12 @@ __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restric
     }
 }
 
-// Steps i0 .. i1-1 (minor: no pdhg_* / reflected_* outputs) of instance blockIdx.x.
-template <typename T>
+// Steps i0 .. i1-1 (minor: no pdhg_* / reflected_* outputs) of instance blockIdx.x:
+// POp runs on the rows of A' (columns), DOp on the rows of A; both carry the step
+// index in k_offset.
+template <class POp, class DOp>
 __global__ void __launch_bounds__(kTinyThreads)
-    tiny_steps_kernel(PrimalOp<T, false, kTinyThreads> pop, DualOp<T, false, kTinyThreads> dop,
+    tiny_steps_kernel(POp pop, DOp dop,
                       const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
                       const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
                       const int32_t* __restrict__ col_off, const int32_t* __restrict__ row_off,
@@ -70,9 +71,9 @@ __global__ void __launch_bounds__(kTinyThreads)
     for (int32_t i = i0; i < i1; ++i) {
         pop.k_offset = i;
         dop.k_offset = i;
-        tiny_pass(pop, rp_t, ci_t, c0, c1, p);  // A'z, primal_step! and dual_y_step!
+        tiny_pass(pop, rp_t, ci_t, c0, c1, p);  // the A'-side pass (primal update)
         __syncthreads();
-        tiny_pass(dop, rp_a, ci_a, r0, r1, p);  // A x_bar and dual_z_step!
+        tiny_pass(dop, rp_a, ci_a, r0, r1, p);  // the A-side pass (dual update)
         __syncthreads();
     }
 }
