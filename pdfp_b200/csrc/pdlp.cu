@@ -259,6 +259,13 @@ class LpSolver {
         ProblemIn in{A.m, A.n, A.m > 0 ? A.row_ptr : &zero_rp, A.col_idx, A.val, nullptr};
         std::string msg = build_layout({in}, false, M_.L);  // caller order: no permutation
         if (!msg.empty()) throw Error(E_INVALID, msg);
+        // as for the projector: below 2^18 nonzeros (PDFP_MIXED_MIN_NNZ overrides)
+        // every launch is latency-bound and the mixed form computes in FP64
+        if (f32_) {
+            const char* mm = std::getenv("PDFP_MIXED_MIN_NNZ");
+            const int64_t min_nnz = mm ? std::atoll(mm) : (int64_t(1) << 18);
+            if (M_.L.NNZ < min_nnz) f32_ = false;
+        }
         M_.upload(ar_, f32_);
         {
             const char* te = std::getenv("PDFP_TINY");
