@@ -283,16 +283,19 @@ def main():
                            precision=precision)
         tun = (gpu.C.c_int32 * 8)()
         gpu.L.check(gpu.L.lib().pdfp_get_tuning(st._h, tun))
+        stg = (gpu.C.c_int32 * 2)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_stages(st._h, stg))
         tuning = {"a_t_stage_bytes": tun[0], "a_t_threads": tun[1], "a_t_tiles": tun[2],
-                  "a_stage_bytes": tun[3], "a_threads": tun[4], "a_tiles": tun[5],
-                  "a_t_gather_l2": tun[6], "a_gather_l2": tun[7]}
+                  "a_t_stages": stg[0], "a_stage_bytes": tun[3], "a_threads": tun[4],
+                  "a_tiles": tun[5], "a_stages": stg[1], "a_t_gather_l2": tun[6],
+                  "a_gather_l2": tun[7]}
         tms = (gpu.C.c_float * 64)()
-        tcfg = (gpu.C.c_int32 * 256)()
+        tcfg = (gpu.C.c_int32 * 320)()
         cnt = gpu.C.c_int32()
         gpu.L.check(gpu.L.lib().pdfp_get_tuning_table(st._h, tms, tcfg, 64, gpu.C.byref(cnt)))
         for i in range(cnt.value):
-            log(f"[bench]   tune side={'A' if tcfg[4*i] else 'At'} stage={tcfg[4*i+1]} "
-                f"nt={tcfg[4*i+2]} l2={tcfg[4*i+3]}: {tms[i]*1e3:.1f} us")
+            log(f"[bench]   tune side={'A' if tcfg[5*i] else 'At'} stage={tcfg[5*i+1]} "
+                f"nt={tcfg[5*i+2]} l2={tcfg[5*i+3]} stages={tcfg[5*i+4]}: {tms[i]*1e3:.1f} us")
         log(f"[bench] {precision} handle built in {time.time() - t:.1f}s, tuning {tuning}")
         run_projections(st, sc, warm, params, False)
         gpu.L.check(gpu.L.lib().pdfp_set_kernel_timing(st._h, 1))
@@ -332,18 +335,34 @@ def main():
     value = mx["tot_iters"] / mx["dev_s"]
     peak, peak_kind = measured_hbm_peak()
     roof = None
-    if mx["kp_ms"]:
-        achieved = bytes_primal32 / (mx["kp_ms"] * 1e-3) / 1e9
-        # DRAM bytes of one launch of this kernel on the default workload, from one
-        # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
+    if mx["kp_ms"] and mx["kd_ms"]:
+        # one entry per step kernel; `roofline` is the one that takes longer per launch
+        bytes_dual32 = 8.0 * nnz + 4.0 * (m + 1) + 4.0 * 4 * m + 4.0 * n
+        # DRAM bytes of one launch on the default workload, from ncu captures
+        # (dram__bytes_read.sum + dram__bytes_write.sum)
         default = (args.workload, args.m, args.n, args.nnz) == ("zipf-lp", 1_000_000, 2_000_000,
                                                                 20_000_000)
-        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": 253.1e6 if default else None,
-                "kernel": f"tile_spmv_kernel<PrimalOp<float, false, {mx['tuning']['a_t_threads']}>> (A'z + fused primal/y update)",
-                "peak_kind": peak_kind, "bytes_per_launch": bytes_primal32,
-                "mean_launch_ms": round(mx["kp_ms"], 5),
-                "dual_kernel_mean_launch_ms": round(mx["kd_ms"], 5) if mx["kd_ms"] else None}
+        tun = mx["tuning"]
+
+        def kname(op, threads):
+            return (f"flat_spmv_kernel<{op}<float, false, 256>>" if threads == 0
+                    else f"tile_spmv_kernel<{op}<float, false, {threads}>>")
+
+        entries = []
+        for label, op, threads, ms, byts, traffic in [
+                ("A'z + fused primal/y update", "PrimalOp", tun["a_t_threads"], mx["kp_ms"],
+                 bytes_primal32, 253.1e6),
+                ("A x_bar + fused z update", "DualOp", tun["a_threads"], mx["kd_ms"],
+                 bytes_dual32, 188.2e6)]:
+            achieved = byts / (ms * 1e-3) / 1e9
+            entries.append({"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                            "unit": "GB/s", "frac": round(achieved / peak, 4),
+                            "traffic": traffic if default else None,
+                            "kernel": f"{kname(op, threads)} ({label})", "peak_kind": peak_kind,
+                            "bytes_per_launch": byts, "mean_launch_ms": round(ms, 5)})
+        entries.sort(key=lambda e: -e["mean_launch_ms"])
+        roof = dict(entries[0])
+        roof["other_kernel"] = entries[1]
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -371,18 +390,18 @@ def main():
         line["fp64_reference_form"] = refform_line
         line["speedup_vs_fp64_reference_form"] = round(value / refform_line["value"], 3)
     line["roofline"] = roof
-    if mx["kp_ms"]:
+    if mx["kp_ms"] and mx["kd_ms"]:
         # the ceiling that binds a scattered sparsity pattern: random 4-byte gathers
         grate = gpu.C.c_double()
         gpu.L.check(gpu.L.lib().pdfp_measure_gather_rate((nnz // 4) * 4, m, 20, gpu.C.byref(grate)))
         peak_g = grate.value / 1e9
-        ach_p = nnz / (mx["kp_ms"] * 1e-3) / 1e9
-        ach_d = nnz / (mx["kd_ms"] * 1e-3) / 1e9 if mx["kd_ms"] else None
+        ach = {"PrimalOp": nnz / (mx["kp_ms"] * 1e-3) / 1e9, "DualOp": nnz / (mx["kd_ms"] * 1e-3) / 1e9}
+        dom = "PrimalOp" if mx["kp_ms"] >= mx["kd_ms"] else "DualOp"
         line["gather_roofline"] = {
             "bound": "random 4-byte gathers", "unit": "Ggathers/s", "peak": round(peak_g, 1),
-            "achieved": round(ach_p, 1), "frac": round(ach_p / peak_g, 4),
-            "dual_kernel_achieved": round(ach_d, 1) if ach_d else None,
-            "dual_kernel_frac": round(ach_d / peak_g, 4) if ach_d else None,
+            "kernel": dom, "achieved": round(ach[dom], 1), "frac": round(ach[dom] / peak_g, 4),
+            "per_kernel": {k: {"achieved": round(v, 1), "frac": round(v / peak_g, 4)}
+                           for k, v in ach.items()},
             "peak_source": "pdfp_measure_gather_rate on this GPU (streamed indices, "
                            f"{(nnz // 4) * 4} gathers from a {m}-entry FP32 vector)"}
     h2d = 8 * n * args.steps

@@ -188,16 +188,21 @@ PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
  * PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size, and
  * PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the engine with its default
  * settings (flat1: the flat engine's one-quad-per-thread variant), and
- * PDFP_TUNING="s,t,l,s,t,l" pins both sides for handles created while it is
- * set: stage bytes, threads per role and the L2-only flag of A', then of A,
- * with the values out[] below reports.
+ * PDFP_TUNING="s,t,l,s,t,l[,n,n]" pins both sides for handles created while it
+ * is set: stage bytes, threads per role and the L2-only flag of A', then of A,
+ * with the values out[] below reports, and optionally the stage counts of A'
+ * and A (pdfp_get_tuning_stages; default 4).
  * out[8] = {A' stage bytes, A' threads per role (0: flat engine), A' tiles,
  * A stage bytes, A threads per role (0: flat engine), A tiles,
  * A' gathers L2-only, A gathers L2-only}. */
 PDFP_API int pdfp_get_tuning(const pdfp_handle* h, int32_t* out);
+/* Shared-memory stages per block of the tile engine on each side: out[2] =
+ * {A', A} (2..4; 4 for the flat engine, which has none). */
+PDFP_API int pdfp_get_tuning_stages(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
- * launch time, cfg[4i..4i+3] = {side (0: A', 1: A), stage bytes, threads per
- * role (0: flat engine), gathers L2-only}; *count receives the number of rows. */
+ * launch time, cfg[5i..5i+4] = {side (0: A', 1: A), stage bytes, threads per
+ * role (0: flat engine), gathers L2-only, stages}; *count receives the number
+ * of rows. */
 PDFP_API int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
                                    int32_t* count);
 

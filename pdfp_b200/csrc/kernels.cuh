@@ -18,7 +18,7 @@ namespace pdfp {
 template <class Op>
 size_t tile_dyn_smem(const SideDev& s) {
     size_t nv = Op::NV > 0 ? Op::NV : 1;
-    return kStages * static_cast<size_t>(s.stage_bytes) +
+    return static_cast<size_t>(s.stages) * static_cast<size_t>(s.stage_bytes) +
            ((nv * s.max_tile_rows * sizeof(typename Op::AT) + 127) & ~size_t(127));
 }
 

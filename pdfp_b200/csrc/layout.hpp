@@ -81,6 +81,7 @@ struct alignas(32) ChunkDesc {
 struct SideDev {
     int32_t rows;
     int32_t n_tiles, n_chunks, max_tile_rows, stage_bytes;
+    int32_t stages = 4;  // shared-memory stages per block of the tile engine (2..4)
     const int32_t* rp;
     const int32_t* ci;
     const int32_t* tile_row;     // n_tiles + 1

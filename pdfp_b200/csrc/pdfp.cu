@@ -501,9 +501,13 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     // reports them; the tuner does not run.
     bool pinned = false;
     if (const char* pt = std::getenv("PDFP_TUNING")) {
-        int v[6];
-        if (std::sscanf(pt, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) != 6)
-            throw Error(E_INVALID, "PDFP_TUNING must read stage,threads,l2,stage,threads,l2");
+        int v[8] = {0, 0, 0, 0, 0, 0, 4, 4};
+        const int got = std::sscanf(pt, "%d,%d,%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4],
+                                    &v[5], &v[6], &v[7]);
+        if (got != 6 && got != 8)
+            throw Error(E_INVALID, "PDFP_TUNING must read stage,threads,l2,stage,threads,l2[,stages,stages]");
+        if (v[6] < 2 || v[6] > 4 || v[7] < 2 || v[7] > 4)
+            throw Error(E_INVALID, "PDFP_TUNING: stages must be 2, 3 or 4");
         StepSide* sides[2][2] = {{&p32_, &d32_}, {&p64_, &d64_}};
         for (int k = 0; k < 2; ++k)
             for (int f = 0; f < 2; ++f) {
@@ -519,6 +523,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
                 q.stage_bytes = c[0] > 0 ? c[0] : q.stage_bytes;
                 q.nt = c[1] == 0 ? 256 : c[1];
                 q.gather_l2 = c[2] != 0;
+                q.stages = v[6 + k];
             }
         pinned = true;
     }
@@ -595,6 +600,7 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     }
     StageGeom g{e, e, e, primal ? 8 : 3, 1, s.stage_bytes, 2048};
     s.tiling = M_.make_tiling(ar_, primal, g);
+    s.tiling.dev.stages = s.stages;
     if (primal)
         s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_)
                      : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_);
@@ -609,15 +615,21 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
 // all-zero state, which it resets afterwards.
 void Projector::autotune(bool f32) {
     struct Cand {
-        int engine, stage, nt, l2, qpt;
+        int engine, stage, nt, l2, qpt, stages;
     };
     // tile engine, 4 stages per block: 12-16 KB stages give 3-4 blocks per SM, 24 KB
-    // two, 32-48 KB one; then the flat engine with both gather cache policies
+    // two, 32-48 KB one; 128-thread roles with 2-3 larger stages, 3 blocks per SM;
+    // then the flat engine with both gather cache policies
     static const Cand cands[] = {
-        {0, 12 * 1024, 128, 0, 0}, {0, 16 * 1024, 128, 0, 0}, {0, 16 * 1024, 256, 0, 0},
-        {0, 24 * 1024, 256, 0, 0}, {0, 32 * 1024, 256, 0, 0}, {0, 48 * 1024, 256, 0, 0},
-        {0, 16 * 1024, 256, 1, 0}, {0, 24 * 1024, 256, 1, 0}, {0, 32 * 1024, 256, 1, 0},
-        {1, 0, 0, 0, 2},           {1, 0, 0, 0, 1},           {1, 0, 0, 1, 2}};
+        {0, 12 * 1024, 128, 0, 0, 4}, {0, 16 * 1024, 128, 0, 0, 4}, {0, 16 * 1024, 256, 0, 0, 4},
+        {0, 24 * 1024, 256, 0, 0, 4}, {0, 32 * 1024, 256, 0, 0, 4}, {0, 48 * 1024, 256, 0, 0, 4},
+        {0, 16 * 1024, 256, 1, 0, 4}, {0, 24 * 1024, 256, 1, 0, 4}, {0, 32 * 1024, 256, 1, 0, 4},
+        {0, 24 * 1024, 128, 1, 0, 3}, {0, 32 * 1024, 128, 1, 0, 2}, {0, 24 * 1024, 128, 0, 0, 3},
+        {0, 12 * 1024, 128, 0, 0, 3}, {0, 12 * 1024, 128, 0, 0, 2}, {0, 16 * 1024, 128, 0, 0, 3},
+        {0, 16 * 1024, 128, 1, 0, 3}, {0, 20 * 1024, 128, 1, 0, 3}, {0, 20 * 1024, 128, 0, 0, 3},
+        {0, 24 * 1024, 128, 1, 0, 2}, {0, 28 * 1024, 128, 1, 0, 2}, {0, 16 * 1024, 128, 0, 0, 2},
+        {0, 14 * 1024, 128, 0, 0, 3}, {0, 18 * 1024, 128, 0, 0, 3}, {0, 32 * 1024, 128, 1, 0, 3},
+        {1, 0, 0, 0, 2, 4},           {1, 0, 0, 0, 1, 4},           {1, 0, 0, 1, 2, 4}};
     constexpr int NC = sizeof(cands) / sizeof(cands[0]);
     cudaEvent_t e0, e1;
     PDFP_CK(cudaEventCreate(&e0));
@@ -630,6 +642,7 @@ void Projector::autotune(bool f32) {
         bool empty_side = false;
         for (int i = 0; i < NC; ++i) {
             sides[i].engine = cands[i].engine;
+            sides[i].stages = cands[i].stages;
             if (cands[i].engine == 1) sides[i].qpt = cands[i].qpt;
             sides[i].stage_bytes = cands[i].stage;
             sides[i].nt = cands[i].nt;
@@ -668,7 +681,7 @@ void Projector::autotune(bool f32) {
         }
         int bi = 0;
         for (int i = 0; i < NC; ++i) {
-            tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, best_ms[i]});
+            tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, cands[i].stages, best_ms[i]});
             if (best_ms[i] < best_ms[bi]) bi = i;
         }
         dst = sides[bi];
@@ -690,12 +703,19 @@ int Projector::tuning_table(float* ms, int32_t* cfg, int cap) const {
     const int n = static_cast<int>(tune_table_.size());
     for (int i = 0; i < n && i < cap; ++i) {
         ms[i] = tune_table_[i].ms;
-        cfg[4 * i + 0] = tune_table_[i].side;
-        cfg[4 * i + 1] = tune_table_[i].stage;
-        cfg[4 * i + 2] = tune_table_[i].nt;
-        cfg[4 * i + 3] = tune_table_[i].l2;
+        cfg[5 * i + 0] = tune_table_[i].side;
+        cfg[5 * i + 1] = tune_table_[i].stage;
+        cfg[5 * i + 2] = tune_table_[i].nt;
+        cfg[5 * i + 3] = tune_table_[i].l2;
+        cfg[5 * i + 4] = tune_table_[i].stages;
     }
     return n;
+}
+
+void Projector::tuning_stages(int32_t* out) const {
+    const bool f32 = precision_ == PDFP_MIXED;
+    out[0] = (f32 ? p32_ : p64_).stages;
+    out[1] = (f32 ? d32_ : d64_).stages;
 }
 
 void Projector::tuning(int32_t* out) const {

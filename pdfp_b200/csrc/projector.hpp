@@ -50,6 +50,7 @@ class Projector {
     // Chosen step-kernel configurations: {stage_bytes, threads, tiles} for the
     // A'-side and the A-side kernel of the handle's base precision.
     void tuning(int32_t* out) const;
+    void tuning_stages(int32_t* out) const;
     // Every autotuner measurement: ms[i] and cfg[4i..4i+3] = {side (0: A', 1: A),
     // stage bytes, threads per role, gathers cached in L2 only}; returns the count.
     int tuning_table(float* ms, int32_t* cfg, int cap) const;
@@ -60,6 +61,7 @@ class Projector {
     struct StepSide {
         int engine = 0;  // 0: tile engine (tile_spmv.cuh), 1: flat engine (flat_spmv.cuh)
         int qpt = 2;     // flat engine: quads (4 nonzeros) per thread and tile, 1 or 2
+        int stages = 4;  // tile engine: shared-memory stages per block, 2..4
         int stage_bytes = 32 * 1024;
         int nt = 256;
         DeviceMatrix::Tiling tiling;
@@ -69,6 +71,7 @@ class Projector {
     };
     struct TuneRow {
         int side, stage, nt, l2;  // nt = 0: the flat engine
+        int stages;
         float ms;
     };
     std::vector<TuneRow> tune_table_;

@@ -41,7 +41,7 @@
 
 namespace pdfp {
 
-constexpr int kStages = 4;     // shared-memory stages per block
+constexpr int kStages = 4;     // most shared-memory stages per block (SideDev::stages: 2..4)
 constexpr int kReduceBar = 2;  // named barrier id of the reducer threads
 
 // Where each region of a chunk lives inside a stage buffer.
@@ -133,7 +133,8 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     constexpr int UNROLL = sizeof(MT) == 4 ? 16 : 8;  // scalar path: gathers in flight per thread
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     __shared__ TileKernelSmem<Op> sh;
-    AT* rowsum = reinterpret_cast<AT*>(dyn_smem + kStages * (size_t)s.stage_bytes);  // [NV][max_rows]
+    const int NS = s.stages;  // stages in use
+    AT* rowsum = reinterpret_cast<AT*>(dyn_smem + NS * (size_t)s.stage_bytes);  // [NV][max_rows]
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < kStages; ++i) {
@@ -151,9 +152,9 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         if (threadIdx.x == 2 * NT) {
             WorkIter it{-1, 0, 0};
             for (uint32_t u = 0;; ++u) {
-                const int st = u % kStages;
-                if (u >= kStages &&
-                    !mbar_wait_bounded(&sh.empty[st], ((u / kStages) - 1) & 1u, op.err())) {
+                const int st = u % NS;
+                if (u >= (uint32_t)NS &&
+                    !mbar_wait_bounded(&sh.empty[st], ((u / NS) - 1) & 1u, op.err())) {
                     sh.flag = 1;  // the stage was never released: stop feeding
                     sh.stage_chunk[st] = -1;
                     mbar_arrive(&sh.full[st]);
@@ -175,11 +176,11 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         // ---- gatherers: products of each chunk, in place over its values ----
         const int g = threadIdx.x;
         for (uint32_t u = 0;; ++u) {
-            const int st = u % kStages;
+            const int st = u % NS;
             // Each gatherer waits and arrives on its own: with no barrier among them a
             // thread whose gathers have landed runs ahead into the next stages while
             // slower gathers of the previous one are still in flight.
-            const bool ok = mbar_wait_bounded(&sh.full[st], (u / kStages) & 1u, op.err());
+            const bool ok = mbar_wait_bounded(&sh.full[st], (u / NS) & 1u, op.err());
             if (!ok) sh.flag = 1;
             const int32_t c = ok ? sh.stage_chunk[st] : -1;
             if (c >= 0 && NV > 0) {
@@ -277,8 +278,8 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     int32_t cur_tile = -1;
 
     for (uint32_t u = 0;; ++u) {
-        const int st = u % kStages;
-        if (!group_wait(&sh.prod[st], (u / kStages) & 1u, op.err(), r == 0, kReduceBar, NT, &sh.flag))
+        const int st = u % NS;
+        if (!group_wait(&sh.prod[st], (u / NS) & 1u, op.err(), r == 0, kReduceBar, NT, &sh.flag))
             break;  // a wait gave up (error recorded)
         const int32_t c = sh.stage_chunk[st];
         if (c < 0) break;
