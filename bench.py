@@ -185,14 +185,16 @@ def flip_targets(xt, I, milp, rng, frac=0.05):
     return xt
 
 
-def run_projections(state, sc, xt_seq, params, timed):
-    """Project each target (set_target -> solve -> read x) and collect per-step figures."""
+def run_projections(state, xt_seq, x_out, params, timed):
+    """Project each target as the pump does -- set_target(x_tilde ./ D_c) -> solve ->
+    D_c .* pdhg_x, the scaling on the device -- and collect per-step figures.  The
+    targets and x_out are page-locked host arrays."""
     out = []
     for xt in xt_seq:
         t0 = time.perf_counter()
-        state.set_target(xt / sc.D_c)
+        state.set_target_unscaled(xt)
         state.solve(params, 1.0)
-        x = state.pdhg_x
+        x = state.get_unscaled("pdhg_x", out=x_out)
         t1 = time.perf_counter()
         r = state.last
         out.append({"iters": r["total_count"], "device_ms": r["device_ms"], "wall_s": t1 - t0,
@@ -274,13 +276,20 @@ def main():
     seq = [xt0]
     for _ in range(args.warmup + args.steps - 1):
         seq.append(flip_targets(seq[-1], I, milp, rng))
-    warm, timed = seq[:args.warmup], seq[args.warmup:]
+    pinned = []  # the targets in page-locked host memory, as a caller would stage them
+    for xt in seq:
+        a = gpu.pinned_zeros(len(xt))
+        a[:] = xt
+        pinned.append(a)
+    x_out = gpu.pinned_zeros(len(xt0))
+    warm, timed = pinned[:args.warmup], pinned[args.warmup:]
 
     results = {}
     for precision in (["mixed"] if args.no_fp64 else ["mixed", "fp64"]):
         t = time.time()
         st = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w,
                            precision=precision)
+        st.set_col_scale(sc.D_c)
         tun = (gpu.C.c_int32 * 8)()
         gpu.L.check(gpu.L.lib().pdfp_get_tuning(st._h, tun))
         stg = (gpu.C.c_int32 * 2)()
@@ -297,11 +306,11 @@ def main():
             log(f"[bench]   tune side={'A' if tcfg[5*i] else 'At'} stage={tcfg[5*i+1]} "
                 f"nt={tcfg[5*i+2]} l2={tcfg[5*i+3]} stages={tcfg[5*i+4]}: {tms[i]*1e3:.1f} us")
         log(f"[bench] {precision} handle built in {time.time() - t:.1f}s, tuning {tuning}")
-        run_projections(st, sc, warm, params, False)
+        run_projections(st, warm, x_out, params, False)
         gpu.L.check(gpu.L.lib().pdfp_set_kernel_timing(st._h, 1))
         barrier(world)
         with ClockSampler(local) as clk:
-            steps = run_projections(st, sc, timed, params, True)
+            steps = run_projections(st, timed, x_out, params, True)
         barrier(world)
         iters = sum(s["iters"] for s in steps)
         dev_s = sum(s["device_ms"] for s in steps) / 1e3
@@ -407,8 +416,9 @@ def main():
     h2d = 8 * n * args.steps
     line["e2e"] = {"value": round(mx["tot_iters"] / mx["wall_s"], 1), "unit": "iters/s",
                    "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
-                   "note": "set_target (host -> device) + solve + pdhg_x (device -> host) per step, "
-                           "host wall clock"}
+                   "note": "set_target_unscaled (page-locked host -> device, x_tilde ./ D_c on "
+                           "the device) + solve + D_c .* pdhg_x (device -> page-locked host) per "
+                           "step, host wall clock"}
     windows = mx["iters"] // 200
     line["gpu_launches"] = int(windows * (2 * 200 + 10) + args.steps * 12)
     line["clocks"] = mx["clocks"]
@@ -451,7 +461,12 @@ def batch_uneven(args, world, rank, local):
         seq = [np.round(rng.random(n))]
         for _ in range(args.warmup + args.steps - 1):
             seq.append(flip_targets(seq[-1], mm.int_idx, mm, rng))
-        seqs.append(seq)
+        pinned = []  # page-locked copies, as a caller would stage them
+        for xt in seq:
+            a = gpu.pinned_zeros(n)
+            a[:] = xt
+            pinned.append(a)
+        seqs.append(pinned)
     params = SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-5,
                               iteration_limit=2_000_000)
     nnz = [p[0].nnz for p in probs]
@@ -462,6 +477,9 @@ def batch_uneven(args, world, rank, local):
     for precision in (["mixed"] if args.no_fp64 else ["mixed", "fp64"]):
         t = time.time()
         bt = gpu.PDFPBatch(probs, precision=precision)
+        for p in range(len(probs)):
+            bt.set_col_scale(p, scs[p].D_c)
+        x_outs = [gpu.pinned_zeros(n) for n in ns]
         log(f"[bench] {precision} batch handle built in {time.time() - t:.1f}s")
         per = []
         for s in range(args.warmup + args.steps):
@@ -470,9 +488,9 @@ def batch_uneven(args, world, rank, local):
                 clk = ClockSampler(local).__enter__()
             w0 = time.perf_counter()
             for p in range(len(probs)):
-                bt.set_target(p, seqs[p][s] / scs[p].D_c)
+                bt.set_target_unscaled(p, seqs[p][s])
             bt.solve(params, 1.0)
-            xs = [bt.get(p, "pdhg_x") for p in range(len(probs))]
+            xs = [bt.get_unscaled(p, "pdhg_x", out=x_outs[p]) for p in range(len(probs))]
             w1 = time.perf_counter()
             its = [r["total_count"] for r in bt.results]
             per.append({"iters": sum(its), "its": its, "device_ms": bt.results[0]["device_ms"],

@@ -171,6 +171,31 @@ PDFP_API int pdfp_solve_batch(pdfp_handle* h, const pdfp_params* params, const d
 PDFP_API int pdfp_get_vector(pdfp_handle* h, int32_t instance, int32_t which, double* out);
 /* s.pdhg_x of an instance: the projection in scaled units (src/pump.jl:338). */
 PDFP_API int pdfp_get_x(pdfp_handle* h, int32_t instance, double* x_scaled);
+
+/* ---- the pump's column scaling on the device (src/pump.jl:300-354) ----------
+ * The pump feeds the projector x ./ D_c and x_tilde ./ D_c and reads back
+ * D_c .* s.pdhg_x (src/pump.jl:305-306, 331, 338, 354).  After
+ * pdfp_set_col_scale, the *_unscaled calls take and return vectors in the
+ * model's own units and do the division and product on the device, correctly
+ * rounded in FP64: bit-identical to the host arithmetic they replace.
+ * D_c: n entries, positive and finite (E_INVALID otherwise); the unscaled
+ * calls return E_INVALID until it is set for the instance. */
+PDFP_API int pdfp_set_col_scale(pdfp_handle* h, int32_t instance, const double* D_c);
+/* pdfp_set_x(h, instance, x ./ D_c), src/pump.jl:305-306. */
+PDFP_API int pdfp_set_x_unscaled(pdfp_handle* h, int32_t instance, const double* x);
+/* pdfp_set_target(h, instance, x_tilde ./ D_c), src/pump.jl:331. */
+PDFP_API int pdfp_set_target_unscaled(pdfp_handle* h, int32_t instance, const double* x_tilde);
+/* D_c .* (a primal column vector: PDFP_VEC_PDHG_X, _CURRENT_X or _REFLECTED_X). */
+PDFP_API int pdfp_get_vector_unscaled(pdfp_handle* h, int32_t instance, int32_t which, double* out);
+/* D_c .* s.pdhg_x, src/pump.jl:338. */
+PDFP_API int pdfp_get_x_unscaled(pdfp_handle* h, int32_t instance, double* x);
+
+/* Page-locked host memory for the vectors passed to the setters and getters:
+ * host <-> device copies from it run at DMA speed instead of through the
+ * driver's pageable staging.  Any host pointer is accepted by every call;
+ * this is only faster.  Free with pdfp_host_free. */
+PDFP_API int pdfp_host_alloc(int64_t bytes, void** out);
+PDFP_API int pdfp_host_free(void* p);
 /* Instance count, rows and columns of an instance. */
 PDFP_API int pdfp_shape(const pdfp_handle* h, int32_t instance, int32_t* k, int32_t* m, int32_t* n);
 /* Release every device buffer of the handle (the Julia finalizer). */

@@ -99,6 +99,13 @@ SIGNATURES = {
     "pdfp_solve_batch": (C.c_int, [vp, C.POINTER(Params), dp, C.POINTER(Result)]),
     "pdfp_get_vector": (C.c_int, [vp, C.c_int32, C.c_int32, dp]),
     "pdfp_get_x": (C.c_int, [vp, C.c_int32, dp]),
+    "pdfp_set_col_scale": (C.c_int, [vp, C.c_int32, dp]),
+    "pdfp_set_x_unscaled": (C.c_int, [vp, C.c_int32, dp]),
+    "pdfp_set_target_unscaled": (C.c_int, [vp, C.c_int32, dp]),
+    "pdfp_get_vector_unscaled": (C.c_int, [vp, C.c_int32, C.c_int32, dp]),
+    "pdfp_get_x_unscaled": (C.c_int, [vp, C.c_int32, dp]),
+    "pdfp_host_alloc": (C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
+    "pdfp_host_free": (C.c_int, [C.c_void_p]),
     "pdfp_shape": (C.c_int, [vp, C.c_int32, ip, ip, ip]),
     "pdfp_destroy": (C.c_int, [vp]),
     "pdfp_set_kernel_timing": (C.c_int, [vp, C.c_int32]),

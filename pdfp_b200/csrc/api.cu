@@ -2,6 +2,7 @@
 //
 // Every entry point catches the library's exceptions and returns a status
 // code; the message is kept per thread for pdfp_last_error().
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -181,6 +182,52 @@ int pdfp_get_vector(pdfp_handle* h, int32_t instance, int32_t which, double* out
 
 int pdfp_get_x(pdfp_handle* h, int32_t instance, double* x_scaled) {
     return pdfp_get_vector(h, instance, PDFP_VEC_PDHG_X, x_scaled);
+}
+
+int pdfp_set_col_scale(pdfp_handle* h, int32_t instance, const double* D_c) {
+    return guarded([&] {
+        if (!h || !D_c) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->set_col_scale(instance, D_c);
+    });
+}
+
+int pdfp_set_x_unscaled(pdfp_handle* h, int32_t instance, const double* x) {
+    return guarded([&] {
+        if (!h || !x) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->set_x(instance, x, true);
+    });
+}
+
+int pdfp_set_target_unscaled(pdfp_handle* h, int32_t instance, const double* x_tilde) {
+    return guarded([&] {
+        if (!h || !x_tilde) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->set_target(instance, x_tilde, true);
+    });
+}
+
+int pdfp_get_vector_unscaled(pdfp_handle* h, int32_t instance, int32_t which, double* out) {
+    return guarded([&] {
+        if (!h || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->get_vector(instance, which, out, true);
+    });
+}
+
+int pdfp_get_x_unscaled(pdfp_handle* h, int32_t instance, double* x) {
+    return pdfp_get_vector_unscaled(h, instance, PDFP_VEC_PDHG_X, x);
+}
+
+int pdfp_host_alloc(int64_t bytes, void** out) {
+    return guarded([&] {
+        if (!out || bytes < 0) throw pdfp::Error(PDFP_E_INVALID, "bad argument");
+        *out = nullptr;
+        PDFP_CK(cudaMallocHost(out, static_cast<size_t>(std::max<int64_t>(bytes, 1))));
+    });
+}
+
+int pdfp_host_free(void* p) {
+    return guarded([&] {
+        if (p) PDFP_CK(cudaFreeHost(p));
+    });
 }
 
 int pdfp_shape(const pdfp_handle* h, int32_t instance, int32_t* k, int32_t* m, int32_t* n) {

@@ -284,6 +284,60 @@ struct PermuteOut {
     __device__ void elem(int, int32_t j) const { dst[orig[j]] = static_cast<double>(src[j]); }
 };
 
+// Unscaled caller vector -> scaled packed vector: dst[j] = src[caller index of j] / D_c[j],
+// the pump's x_tilde ./ D_c (src/pump.jl:331; x ./ D_c at 305-306) done on the
+// device.  Both operands are FP64 and the quotient is correctly rounded, so the
+// result equals the host's division bit for bit.
+template <typename T>
+struct ScaleIn {
+    T* dst;
+    T* dst2;  // optional second destination
+    const double* src;
+    const double* dc;  // D_c in packed order
+    const int32_t *off, *orig;
+    int32_t only;
+    __device__ bool active(int p) const { return p == only; }
+    __device__ int32_t begin(int p) const { return off[p]; }
+    __device__ int32_t end(int p) const { return off[p + 1]; }
+    __device__ void elem(int, int32_t j) const {
+        const T x = static_cast<T>(__ddiv_rn(src[orig[j]], dc[j]));
+        dst[j] = x;
+        if (dst2) dst2[j] = x;
+    }
+};
+
+// Scaled packed vector -> unscaled caller vector: dst[caller index of j] = D_c[j] * src[j],
+// the pump's D_c .* s.pdhg_x (src/pump.jl:338) done on the device (one correctly
+// rounded FP64 product, as on the host).
+template <typename T>
+struct ScaleOut {
+    double* dst;
+    const T* src;
+    const double* dc;
+    const int32_t *off, *orig;
+    int32_t only;
+    __device__ bool active(int p) const { return p == only; }
+    __device__ int32_t begin(int p) const { return off[p]; }
+    __device__ int32_t end(int p) const { return off[p + 1]; }
+    __device__ void elem(int, int32_t j) const {
+        dst[orig[j]] = __dmul_rn(dc[j], static_cast<double>(src[j]));
+    }
+};
+
+// *nan_seen = 1 when the staged caller vector of instance `only` holds a NaN
+struct NanScan {
+    const double* src;
+    const int32_t* off;
+    int32_t only;
+    int32_t* nan_seen;
+    __device__ bool active(int p) const { return p == only; }
+    __device__ int32_t begin(int) const { return 0; }
+    __device__ int32_t end(int p) const { return off[p + 1] - off[p]; }
+    __device__ void elem(int, int32_t i) const {
+        if (isnan(src[i])) *nan_seen = 1;
+    }
+};
+
 template <typename S, typename D>
 struct ConvertVecs {  // the live iterate set of instance `only`: S -> D
     IterVecs<S> s;
@@ -392,9 +446,12 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     st_ = ar_.alloc<InstState>(K_);
     flags_ = ar_.alloc<InstFlags>(K_ + 1);
     err_ = ar_.alloc<int32_t>(4);
+    nan_seen_ = ar_.alloc<int32_t>(1);
+    has_col_scale_.assign(K_, false);
     sp_ = ar_.alloc<SolveParams>(K_);
     stage_ = ar_.alloc<double>(std::max<int64_t>(std::max(M_.max_m, M_.max_n), 1));
     PDFP_CK(cudaMallocHost(&flags_h_, sizeof(InstFlags) * (K_ + 1)));
+    PDFP_CK(cudaMallocHost(&nan_seen_h_, sizeof(int32_t)));
     vec_mode_.assign(K_, precision_ == PDFP_MIXED ? MODE_FP32 : MODE_FP64);
 
     // per-instance data vectors (permuted into packed order)
@@ -738,6 +795,7 @@ Projector::~Projector() {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     graphs_.clear();
     if (flags_h_) cudaFreeHost(flags_h_);
+    if (nan_seen_h_) cudaFreeHost(nan_seen_h_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -745,32 +803,68 @@ void Projector::check_instance(int p) const {
     if (p < 0 || p >= K_) throw Error(E_INVALID, "instance index out of range");
 }
 
-void Projector::set_x(int p, const double* x) {
-    check_instance(p);
-    const HostLayout& L = M_.L;
-    const int32_t n = L.col_off[p + 1] - L.col_off[p];
-    if (n == 0) return;
-    PDFP_CK(cudaMemcpyAsync(stage_, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
-    if (vec_mode_[p] == MODE_FP32)
-        launch_elem(K_, n, PermuteIn<float>{v32_.cx, v32_.ix, stage_, M_.col_off, M_.col_orig, p}, stream_);
-    else
-        launch_elem(K_, n, PermuteIn<double>{v64_.cx, v64_.ix, stage_, M_.col_off, M_.col_orig, p}, stream_);
+// Stage the caller's column vector of instance p (n values) and raise E_INVALID,
+// before anything is written, when it holds a NaN.
+void Projector::stage_cols(int p, const double* src, const char* what) {
+    const int32_t n = M_.L.col_off[p + 1] - M_.L.col_off[p];
+    PDFP_CK(cudaMemcpyAsync(stage_, src, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    PDFP_CK(cudaMemsetAsync(nan_seen_, 0, sizeof(int32_t), stream_));
+    launch_elem(K_, n, NanScan{stage_, M_.col_off, p, nan_seen_}, stream_);
     PDFP_CK(cudaGetLastError());
+    PDFP_CK(cudaMemcpyAsync(nan_seen_h_, nan_seen_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    PDFP_CK(cudaStreamSynchronize(stream_));
+    if (*nan_seen_h_) throw Error(E_INVALID, std::string("NaN in the ") + what);
+}
+
+// Write the staged vector into dst (and dst2) in packed order: as given, or divided by D_c.
+template <typename T>
+void Projector::load_cols(int p, T* dst, T* dst2, bool unscaled) {
+    const int32_t n = M_.L.col_off[p + 1] - M_.L.col_off[p];
+    if (unscaled)
+        launch_elem(K_, n, ScaleIn<T>{dst, dst2, stage_, col_scale_, M_.col_off, M_.col_orig, p}, stream_);
+    else
+        launch_elem(K_, n, PermuteIn<T>{dst, dst2, stage_, M_.col_off, M_.col_orig, p}, stream_);
+    PDFP_CK(cudaGetLastError());
+}
+
+void Projector::check_unscaled(int p) const {
+    if (!has_col_scale_[p]) throw Error(E_INVALID, "no column scale set for this instance");
+}
+
+void Projector::set_col_scale(int p, const double* dc) {
+    check_instance(p);
+    const int32_t n = cols(p);
+    for (int32_t j = 0; j < n; ++j)
+        if (!(dc[j] > 0.0) || !std::isfinite(dc[j]))
+            throw Error(E_INVALID, "column scale entries must be positive and finite");
+    if (!col_scale_) col_scale_ = ar_.alloc<double>(std::max<int64_t>(M_.L.N, 1));
+    if (n > 0) {
+        PDFP_CK(cudaMemcpyAsync(stage_, dc, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+        load_cols<double>(p, col_scale_, nullptr, false);
+        PDFP_CK(cudaStreamSynchronize(stream_));
+    }
+    has_col_scale_[p] = true;
+}
+
+void Projector::set_x(int p, const double* x, bool unscaled) {
+    check_instance(p);
+    if (unscaled) check_unscaled(p);
+    if (cols(p) == 0) return;
+    stage_cols(p, x, "start point");
+    if (vec_mode_[p] == MODE_FP32)
+        load_cols<float>(p, v32_.cx, v32_.ix, unscaled);
+    else
+        load_cols<double>(p, v64_.cx, v64_.ix, unscaled);
     PDFP_CK(cudaStreamSynchronize(stream_));
 }
 
-void Projector::set_target(int p, const double* xt) {
+void Projector::set_target(int p, const double* xt, bool unscaled) {
     check_instance(p);
-    const HostLayout& L = M_.L;
-    const int32_t n = L.col_off[p + 1] - L.col_off[p];
-    if (n > 0) {
-        for (int32_t j = 0; j < n; ++j)
-            if (std::isnan(xt[j])) throw Error(E_INVALID, "NaN in the target");
-        PDFP_CK(cudaMemcpyAsync(stage_, xt, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
-        launch_elem(K_, n, PermuteIn<double>{v64_.xt, nullptr, stage_, M_.col_off, M_.col_orig, p}, stream_);
-        if (precision_ == PDFP_MIXED)
-            launch_elem(K_, n, PermuteIn<float>{v32_.xt, nullptr, stage_, M_.col_off, M_.col_orig, p}, stream_);
-        PDFP_CK(cudaGetLastError());
+    if (unscaled) check_unscaled(p);
+    if (cols(p) > 0) {
+        stage_cols(p, xt, "target");
+        load_cols<double>(p, v64_.xt, nullptr, unscaled);
+        if (precision_ == PDFP_MIXED) load_cols<float>(p, v32_.xt, nullptr, unscaled);
     }
     warm_start(p);
 }
@@ -788,10 +882,15 @@ void Projector::warm_start(int p) {
     PDFP_CK(cudaStreamSynchronize(stream_));
 }
 
-void Projector::get_vector(int p, int which, double* out) {
+void Projector::get_vector(int p, int which, double* out, bool unscaled) {
     check_instance(p);
     const HostLayout& L = M_.L;
     const bool rowvec = (which == PDFP_VEC_PDHG_Z || which == PDFP_VEC_CURRENT_Z);
+    if (unscaled) {
+        check_unscaled(p);
+        if (rowvec || which == PDFP_VEC_CURRENT_Y || which == PDFP_VEC_PDHG_Y || which == PDFP_VEC_DUAL_SLACK)
+            throw Error(E_INVALID, "only primal column vectors have an unscaled form");
+    }
     const int32_t len = rowvec ? L.row_off[p + 1] - L.row_off[p] : L.col_off[p + 1] - L.col_off[p];
     if (len == 0) return;
     auto pick = [&](auto& v) -> decltype(v.px) {
@@ -809,7 +908,11 @@ void Projector::get_vector(int p, int which, double* out) {
     };
     const int32_t* off = rowvec ? M_.row_off : M_.col_off;
     const int32_t* orig = rowvec ? M_.row_orig : M_.col_orig;
-    if (vec_mode_[p] == MODE_FP32)
+    if (unscaled && vec_mode_[p] == MODE_FP32)
+        launch_elem(K_, len, ScaleOut<float>{stage_, pick(v32_), col_scale_, off, orig, p}, stream_);
+    else if (unscaled)
+        launch_elem(K_, len, ScaleOut<double>{stage_, pick(v64_), col_scale_, off, orig, p}, stream_);
+    else if (vec_mode_[p] == MODE_FP32)
         launch_elem(K_, len, PermuteOut<float>{stage_, pick(v32_), off, orig, p}, stream_);
     else
         launch_elem(K_, len, PermuteOut<double>{stage_, pick(v64_), off, orig, p}, stream_);

@@ -39,11 +39,14 @@ class Projector {
     int rows(int p) const { return M_.L.row_off[p + 1] - M_.L.row_off[p]; }
     int cols(int p) const { return M_.L.col_off[p + 1] - M_.L.col_off[p]; }
 
-    void set_x(int p, const double* x);
-    void set_target(int p, const double* xt);
+    // unscaled = true: the vector is in the caller's original units and the
+    // device applies the instance's column scale D_c (set_col_scale) itself
+    void set_col_scale(int p, const double* dc);
+    void set_x(int p, const double* x, bool unscaled = false);
+    void set_target(int p, const double* xt, bool unscaled = false);
     void warm_start(int p);
     void solve(const pdfp_params* params, const double* primal_weights, pdfp_result* results);
-    void get_vector(int p, int which, double* out);
+    void get_vector(int p, int which, double* out, bool unscaled = false);
     void profile_step(int iterations, float* ms_primal, float* ms_dual, double* bytes_primal,
                       double* bytes_dual);
     void set_polish(bool on) { polish_enabled_ = on ? 1 : 0; }
@@ -84,6 +87,10 @@ class Projector {
     void prepare_side(StepSide& s, bool primal, bool f32);
     void autotune(bool f32);
     void check_instance(int p) const;
+    void check_unscaled(int p) const;
+    void stage_cols(int p, const double* src, const char* what);
+    template <typename T>
+    void load_cols(int p, T* dst, T* dst2, bool unscaled);
     void ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance);
     void record_window(int freq, bool with32, bool with64);
     template <typename T>
@@ -109,6 +116,10 @@ class Projector {
     int32_t* err_ = nullptr;
     SolveParams* sp_ = nullptr;
     double* stage_ = nullptr;
+    double* col_scale_ = nullptr;  // D_c in packed column order, once set_col_scale ran
+    std::vector<bool> has_col_scale_;
+    int32_t* nan_seen_ = nullptr;
+    int32_t* nan_seen_h_ = nullptr;
     std::vector<int> vec_mode_;
     std::vector<bool> has_unscale_;
     std::set<int> polished_;

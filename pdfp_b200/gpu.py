@@ -31,6 +31,45 @@ def device_name() -> str:
     return buf.value.decode()
 
 
+class _HostBlock:
+    """One pdfp_host_alloc block; freed when the last array viewing it goes."""
+
+    def __init__(self, nbytes: int):
+        self.ptr = C.c_void_p()
+        L.check(L.lib().pdfp_host_alloc(max(int(nbytes), 1), C.byref(self.ptr)))
+
+    def __del__(self):
+        try:
+            if self.ptr.value:
+                L.lib().pdfp_host_free(self.ptr)
+                self.ptr = C.c_void_p()
+        except Exception:  # noqa: BLE001 (interpreter shutdown)
+            pass
+
+
+def pinned_zeros(n: int) -> np.ndarray:
+    """A float64 array of n zeros in page-locked host memory (pdfp_host_alloc).
+
+    Vectors passed to the setters and getters from such an array cross to and from
+    the device at DMA speed; any other array works too, more slowly.
+    """
+    block = _HostBlock(8 * n)
+    raw = (C.c_double * max(n, 1)).from_address(block.ptr.value)
+    raw._block = block  # the numpy view keeps raw, raw keeps the block
+    a = np.frombuffer(raw, dtype=np.float64)[:n]
+    a[:] = 0.0
+    return a
+
+
+def _out(out, size):
+    """The caller's output array (float64, contiguous, at least `size` long) or a new one."""
+    if out is None:
+        return np.zeros(max(size, 1))
+    if out.dtype != np.float64 or not out.flags.c_contiguous or out.size < size:
+        raise ValueError("out must be a contiguous float64 array of the vector's length")
+    return out
+
+
 def _precision_code(precision: str) -> int:
     if precision in ("fp64", "FP64", L.FP64):
         return L.FP64
@@ -114,15 +153,33 @@ class PDFPState:
         self.termination_reason = STATUS_NAMES.get(r.status, str(r.status))
         return self.termination_reason
 
-    def get(self, which: str) -> np.ndarray:
+    def get(self, which: str, out=None) -> np.ndarray:
         size = self.m if which.endswith("_z") else self.n
-        out = np.zeros(max(size, 1))
+        out = _out(out, size)
         L.check(L.lib().pdfp_get_vector(self._h, 0, L.VEC[which], L.dptr(out)))
         return out[:size]
 
     @property
     def pdhg_x(self) -> np.ndarray:
         return self.get("pdhg_x")
+
+    # The pump's column scaling on the device (src/pump.jl:305-306, 331, 338):
+    # after set_col_scale(D_c), these take and return vectors in the model's
+    # own units, bit-identical to x ./ D_c and D_c .* s.pdhg_x on the host.
+    def set_col_scale(self, D_c):
+        L.check(L.lib().pdfp_set_col_scale(self._h, 0, L.dptr(L.f64(D_c))))
+
+    def set_x_unscaled(self, x):
+        L.check(L.lib().pdfp_set_x_unscaled(self._h, 0, L.dptr(L.f64(x))))
+
+    def set_target_unscaled(self, x_tilde):
+        L.check(L.lib().pdfp_set_target_unscaled(self._h, 0, L.dptr(L.f64(x_tilde))))
+        self.total_count = 0
+
+    def get_unscaled(self, which: str = "pdhg_x", out=None) -> np.ndarray:
+        out = _out(out, self.n)
+        L.check(L.lib().pdfp_get_vector_unscaled(self._h, 0, L.VEC[which], L.dptr(out)))
+        return out[:self.n]
 
     def profile_step(self, iterations: int):
         a, b = C.c_float(), C.c_float()
@@ -188,12 +245,27 @@ class PDFPBatch:
         self.results = [r.as_dict() for r in rs]
         return [r["status"] for r in self.results]
 
-    def get(self, p: int, which: str) -> np.ndarray:
+    def get(self, p: int, which: str, out=None) -> np.ndarray:
         m, n = self.shapes[p]
         size = m if which.endswith("_z") else n
-        out = np.zeros(max(size, 1))
+        out = _out(out, size)
         L.check(L.lib().pdfp_get_vector(self._h, p, L.VEC[which], L.dptr(out)))
         return out[:size]
+
+    def set_col_scale(self, p: int, D_c):
+        L.check(L.lib().pdfp_set_col_scale(self._h, p, L.dptr(L.f64(D_c))))
+
+    def set_x_unscaled(self, p: int, x):
+        L.check(L.lib().pdfp_set_x_unscaled(self._h, p, L.dptr(L.f64(x))))
+
+    def set_target_unscaled(self, p: int, x_tilde):
+        L.check(L.lib().pdfp_set_target_unscaled(self._h, p, L.dptr(L.f64(x_tilde))))
+
+    def get_unscaled(self, p: int, which: str = "pdhg_x", out=None) -> np.ndarray:
+        n = self.shapes[p][1]
+        out = _out(out, n)
+        L.check(L.lib().pdfp_get_vector_unscaled(self._h, p, L.VEC[which], L.dptr(out)))
+        return out[:n]
 
 
 class ConstraintChecker:

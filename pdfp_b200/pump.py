@@ -185,6 +185,46 @@ def _perturb(xt, x, milp: MILP, rng, general, is_general, ladder: RestartLadder,
 DEVICE_CHECK_MIN_NNZ = 1 << 16  # smaller matrices are checked on the host
 
 
+class _ColumnScaling:
+    """The projector's column scaling (src/pump.jl:305-306, 331, 338, 354).
+
+    The pump hands the projector x ./ D_c and x_tilde ./ D_c and reads back
+    D_c .* s.pdhg_x.  Projectors that hold D_c themselves (set_col_scale; the
+    library's PDFPState and PDFPBatch) do both on the device, bit-identical to
+    the host arithmetic, which then never touches the n-vector; for any other
+    projector this object does it on the host.  `member` selects a batch member.
+    """
+
+    def __init__(self, projector, D_c, member=None):
+        self.proj, self.D_c, self.member = projector, D_c, member
+        self.device = hasattr(projector, "set_col_scale")
+        if self.device:
+            self._call("set_col_scale", D_c)
+
+    def _call(self, name, *args):
+        f = getattr(self.proj, name)
+        return f(*args) if self.member is None else f(self.member, *args)
+
+    def set_x(self, x):
+        if self.device:
+            self._call("set_x_unscaled", x)
+        else:
+            self._call("set_x", x / self.D_c)
+
+    def set_target(self, xt):
+        if self.device:
+            self._call("set_target_unscaled", xt)
+        else:
+            self._call("set_target", xt / self.D_c)
+
+    def x(self):
+        if self.device:
+            return self._call("get_unscaled", "pdhg_x")
+        if self.member is None:
+            return self.D_c * self.proj.pdhg_x
+        return self.D_c * self.proj.get(self.member, "pdhg_x")
+
+
 def _violation_fn(milp: MILP, solvers):
     """max_violation(milp, .) for the pump loop: on the device (bit-identical) when the
     solvers offer it and the matrix is large enough for the copy of x to pay."""
@@ -317,7 +357,8 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
                                   weights, precision=precision)
     if mixed:
         projector.original_primal_residual(sp_.D_r)
-    projector.set_x(x / D_c)
+    scaling = _ColumnScaling(projector, D_c)
+    scaling.set_x(x)
     primal_weight = math.sqrt(1.0 + (len(int_idx) / m if m > 0 else 0.0))
     gap = gap_start
     tightening_budget = gap_start
@@ -343,14 +384,14 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
 
         # Project x~ onto the LP relaxation (:329-363).
         t = time.time()
-        projector.set_target(xt / D_c)
+        scaling.set_target(xt)
         gap_used = gap
         params = SolverParameters(iteration_limit=projection_iteration_limit,
                                   eps_optimal_relative=gap,
                                   eps_feasible_relative=gap * residual_ratio,
                                   time_limit=remaining())
         projector.solve(params, primal_weight)
-        x = D_c * projector.pdhg_x
+        x = scaling.x()
         inner = projector.total_count
         while (mixed and tightening_budget > 1e-6 and elapsed() < time_limit
                and is_integral(x, int_idx, tol)
@@ -363,7 +404,7 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
                                       time_limit=remaining())
             projector.warm_start()
             projector.solve(params, primal_weight)
-            x = D_c * projector.pdhg_x
+            x = scaling.x()
             inner += projector.total_count
         stats.pdhg_iterations += inner
         if gap > gap_floor:
@@ -528,8 +569,9 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
     ru = (1.0 / sp_.D_r) if mixed else None
     prob = (sp_.A, sp_.con_ub, is_eq, is_int, sp_.var_lb, sp_.var_ub, weights, ru)
     batch = solvers.PDFPBatch([prob] * K, precision=precision)
+    scalings = [_ColumnScaling(batch, D_c, p) for p in range(K)]
     for p in range(K):
-        batch.set_x(p, x / D_c)
+        scalings[p].set_x(x)
     primal_weight = math.sqrt(1.0 + (len(int_idx) / m if m > 0 else 0.0))
     gaps = [gap_start] * K
     budgets = [gap_start] * K
@@ -555,10 +597,10 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
         for p, tr in enumerate(trajs):
             tr.iterations += 1
             tr.since_restart += 1
-            batch.set_target(p, tr.xt / D_c)
+            scalings[p].set_target(tr.xt)
         t = time.time()
         batch.solve([params_for(p, True) for p in range(K)], primal_weight)
-        xs = [D_c * batch.get(p, "pdhg_x") for p in range(K)]
+        xs = [scalings[p].x() for p in range(K)]
         inner = [batch.results[p]["total_count"] for p in range(K)]
         # mixed models: tenfold tighter re-solves (src/pump.jl:343-356), batched
         while mixed and elapsed() < time_limit:
@@ -572,7 +614,7 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
                 batch.warm_start(p)
             batch.solve([params_for(p, p in need) for p in range(K)], primal_weight)
             for p in need:
-                xs[p] = D_c * batch.get(p, "pdhg_x")
+                xs[p] = scalings[p].x()
                 inner[p] += batch.results[p]["total_count"]
         stats.projection_time += time.time() - t
         for p, tr in enumerate(trajs):
