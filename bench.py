@@ -298,11 +298,11 @@ def main():
                   "a_t_stages": stg[0], "a_stage_bytes": tun[3], "a_threads": tun[4],
                   "a_tiles": tun[5], "a_stages": stg[1], "a_t_gather_l2": tun[6],
                   "a_gather_l2": tun[7]}
-        tms = (gpu.C.c_float * 64)()
-        tcfg = (gpu.C.c_int32 * 320)()
+        tms = (gpu.C.c_float * 256)()
+        tcfg = (gpu.C.c_int32 * (5 * 256))()
         cnt = gpu.C.c_int32()
-        gpu.L.check(gpu.L.lib().pdfp_get_tuning_table(st._h, tms, tcfg, 64, gpu.C.byref(cnt)))
-        for i in range(cnt.value):
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_table(st._h, tms, tcfg, 256, gpu.C.byref(cnt)))
+        for i in range(min(cnt.value, 256)):
             log(f"[bench]   tune side={'A' if tcfg[5*i] else 'At'} stage={tcfg[5*i+1]} "
                 f"nt={tcfg[5*i+2]} l2={tcfg[5*i+3]} stages={tcfg[5*i+4]}: {tms[i]*1e3:.1f} us")
         log(f"[bench] {precision} handle built in {time.time() - t:.1f}s, tuning {tuning}")

@@ -208,25 +208,29 @@ PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
 
 /* The step-kernel configuration the autotuner chose at creation.  It times, on
  * the handle's own matrix, the tile engine (shared-memory stage size x threads
- * per role x gather cache policy) and the flat engine (both cache policies) and
+ * per role x gather policy) and the flat engine (both cache policies) and
  * keeps the fastest per side; below 256K nonzeros it keeps the default.
+ * Gather policy: 0 = register gathers cached in L1, 1 = register gathers cached
+ * in L2 only, 2 = per-thread async copies into the shared-memory stage (FP32
+ * steps of the tile engine; the reducers form the products, with the same
+ * roundings in the same order, so results do not depend on the policy).
  * PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size, and
  * PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the engine with its default
  * settings (flat1: the flat engine's one-quad-per-thread variant), and
  * PDFP_TUNING="s,t,l,s,t,l[,n,n]" pins both sides for handles created while it
- * is set: stage bytes, threads per role and the L2-only flag of A', then of A,
+ * is set: stage bytes, threads per role and the gather policy of A', then of A,
  * with the values out[] below reports, and optionally the stage counts of A'
  * and A (pdfp_get_tuning_stages; default 4).
  * out[8] = {A' stage bytes, A' threads per role (0: flat engine), A' tiles,
  * A stage bytes, A threads per role (0: flat engine), A tiles,
- * A' gathers L2-only, A gathers L2-only}. */
+ * A' gather policy, A gather policy}. */
 PDFP_API int pdfp_get_tuning(const pdfp_handle* h, int32_t* out);
 /* Shared-memory stages per block of the tile engine on each side: out[2] =
  * {A', A} (2..4; 4 for the flat engine, which has none). */
 PDFP_API int pdfp_get_tuning_stages(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
  * launch time, cfg[5i..5i+4] = {side (0: A', 1: A), stage bytes, threads per
- * role (0: flat engine), gathers L2-only, stages}; *count receives the number
+ * role (0: flat engine), gather policy, stages}; *count receives the number
  * of rows. */
 PDFP_API int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
                                    int32_t* count);

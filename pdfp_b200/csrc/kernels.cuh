@@ -23,28 +23,43 @@ size_t tile_dyn_smem(const SideDev& s) {
 }
 
 // Persistent grid size for an Op on a side (blocks resident on all SMs).
-template <class Op>
-int tile_grid(const SideDev& s, int num_sms) {
+template <class Op, bool ASYNC>
+int tile_grid_of(const SideDev& s, int num_sms) {
     const size_t smem = tile_dyn_smem<Op>(s);
     // The attribute belongs to the kernel, shared by every tiling launched with
     // it: only ever raise it.
     static size_t attr = 0;
     if (smem > attr) {
-        cudaFuncSetAttribute(tile_spmv_kernel<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(tile_spmv_kernel<Op, ASYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
         attr = smem;
     }
     int blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_spmv_kernel<Op>, 2 * Op::NT + 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_spmv_kernel<Op, ASYNC>, 2 * Op::NT + 32,
+                                                  smem);
     const int per_sm = blocks > 0 ? blocks : 1;
     int g = per_sm * num_sms;
     return g < s.n_tiles ? g : s.n_tiles;
 }
 
+// async: the Op's gathers by per-thread async copies (gather policy 2; ignored for
+// Ops that have no such path)
+template <class Op>
+int tile_grid(const SideDev& s, int num_sms, bool async = false) {
+    if constexpr (kAsyncEligible<Op>)
+        if (async) return tile_grid_of<Op, true>(s, num_sms);
+    return tile_grid_of<Op, false>(s, num_sms);
+}
+
 template <class Op>
 void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream) {
     if (s.n_tiles <= 0 || grid <= 0) return;
-    tile_spmv_kernel<Op><<<grid, 2 * Op::NT + 32, tile_dyn_smem<Op>(s), stream>>>(s, op);
+    if constexpr (kAsyncEligible<Op>)
+        if (op.gather_l2 == 2) {
+            tile_spmv_kernel<Op, true><<<grid, 2 * Op::NT + 32, tile_dyn_smem<Op>(s), stream>>>(s, op);
+            return;
+        }
+    tile_spmv_kernel<Op, false><<<grid, 2 * Op::NT + 32, tile_dyn_smem<Op>(s), stream>>>(s, op);
 }
 
 // ---- launching the flat engine ---------------------------------------------------

@@ -579,7 +579,8 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
                 q.qpt = c[0] == 0 || c[0] == flat_stage_bytes(4, 1024) || c[0] == flat_stage_bytes(8, 1024) ? 1 : 2;
                 q.stage_bytes = c[0] > 0 ? c[0] : q.stage_bytes;
                 q.nt = c[1] == 0 ? 256 : c[1];
-                q.gather_l2 = c[2] != 0;
+                if (c[2] < 0 || c[2] > 2) throw Error(E_INVALID, "PDFP_TUNING: gather policy must be 0, 1 or 2");
+                q.gather_l2 = c[2];
                 q.stages = v[6 + k];
             }
         pinned = true;
@@ -628,13 +629,13 @@ void Projector::launch_dual(const StepSide& s, int k) {
 // Grid of a step Op family for a tiling (sets the shared-memory attribute of
 // both the MAJOR and the minor kernel).
 template <template <typename, bool, int> class OpT, typename T>
-static int step_grid(const SideDev& d, int nt, int sms) {
+static int step_grid(const SideDev& d, int nt, int sms, bool async) {
     if (nt == 256) {
-        tile_grid<OpT<T, false, 256>>(d, sms);
-        return tile_grid<OpT<T, true, 256>>(d, sms);
+        tile_grid<OpT<T, false, 256>>(d, sms, async);
+        return tile_grid<OpT<T, true, 256>>(d, sms, async);
     }
-    tile_grid<OpT<T, false, 128>>(d, sms);
-    return tile_grid<OpT<T, true, 128>>(d, sms);
+    tile_grid<OpT<T, false, 128>>(d, sms, async);
+    return tile_grid<OpT<T, true, 128>>(d, sms, async);
 }
 
 void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
@@ -658,12 +659,13 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     StageGeom g{e, e, e, primal ? 8 : 3, 1, s.stage_bytes, 2048};
     s.tiling = M_.make_tiling(ar_, primal, g);
     s.tiling.dev.stages = s.stages;
+    const bool async = s.gather_l2 == 2;
     if (primal)
-        s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_)
-                     : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_);
+        s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_, async)
+                     : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_, async);
     else
-        s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_)
-                     : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_);
+        s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_, async)
+                     : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_, async);
 }
 
 // The autotuner: times the minor step kernel of each side for every candidate
@@ -686,7 +688,12 @@ void Projector::autotune(bool f32) {
         {0, 16 * 1024, 128, 1, 0, 3}, {0, 20 * 1024, 128, 1, 0, 3}, {0, 20 * 1024, 128, 0, 0, 3},
         {0, 24 * 1024, 128, 1, 0, 2}, {0, 28 * 1024, 128, 1, 0, 2}, {0, 16 * 1024, 128, 0, 0, 2},
         {0, 14 * 1024, 128, 0, 0, 3}, {0, 18 * 1024, 128, 0, 0, 3}, {0, 32 * 1024, 128, 1, 0, 3},
-        {1, 0, 0, 0, 2, 4},           {1, 0, 0, 0, 1, 4},           {1, 0, 0, 1, 2, 4}};
+        {1, 0, 0, 0, 2, 4},           {1, 0, 0, 0, 1, 4},           {1, 0, 0, 1, 2, 4},
+        // gather policy 2: per-thread async copies into the stage (FP32 steps)
+        {0, 16 * 1024, 128, 2, 0, 3}, {0, 16 * 1024, 128, 2, 0, 4}, {0, 24 * 1024, 128, 2, 0, 3},
+        {0, 24 * 1024, 128, 2, 0, 2}, {0, 32 * 1024, 128, 2, 0, 3}, {0, 32 * 1024, 256, 2, 0, 4},
+        {0, 48 * 1024, 256, 2, 0, 4}, {0, 24 * 1024, 256, 2, 0, 4}, {0, 12 * 1024, 128, 2, 0, 4},
+        {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}};
     constexpr int NC = sizeof(cands) / sizeof(cands[0]);
     cudaEvent_t e0, e1;
     PDFP_CK(cudaEventCreate(&e0));
@@ -714,6 +721,7 @@ void Projector::autotune(bool f32) {
         }
         for (int sweep = 0; sweep < 2; ++sweep) {
             for (int i = 0; i < NC; ++i) {
+                if (cands[i].l2 == 2 && !f32) continue;  // FP64 steps have no async policy
                 const StepSide& s = sides[i];
                 auto run = [&](int k) {
                     if (primal) {

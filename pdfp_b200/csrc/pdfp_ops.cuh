@@ -75,7 +75,7 @@ struct PrimalOp {
     const InstState* st;
     int32_t k_offset, mode;
     int32_t* errp;
-    int32_t gather_l2;  // 1: gathers cached in L2 only (ld.global.cg)
+    int32_t gather_l2;  // 1: gathers cached in L2 only (ld.global.cg); 2: async copies (tile engine)
 
     __device__ const T* values() const { return v.val_t; }
     __device__ const T* staged(int k) const {
@@ -98,6 +98,7 @@ struct PrimalOp {
     __device__ void gather(int32_t col, T (&g)[1]) const {
         g[0] = gather_l2 ? __ldcg(v.cz + col) : v.cz[col];
     }
+    __device__ const T* gather_src() const { return v.cz; }
     __device__ void row(int32_t j, int32_t rr, int inst, const TileP& p, const T* const* sv,
                         const T (&s)[1], double*) const {
         const T cx = sv[0][rr], ix = sv[1][rr], cy = sv[2][rr], iy = sv[3][rr];
@@ -155,6 +156,7 @@ struct DualOp {
     __device__ void gather(int32_t col, T (&g)[1]) const {
         g[0] = gather_l2 ? __ldcg(v.rx + col) : v.rx[col];
     }
+    __device__ const T* gather_src() const { return v.rx; }
     __device__ void row(int32_t i, int32_t rr, int inst, const TileP& t, const T* const* sv,
                         const T (&s)[1], double*) const {
         const T cz = sv[0][rr], iz = sv[1][rr], b = sv[2][rr];

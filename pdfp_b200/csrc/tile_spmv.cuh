@@ -36,6 +36,9 @@
 // per-row epilogue; see pdfp_ops.cuh.  Evaluation Ops also reduce per-tile
 // partial sums (FP64, fixed order) into a partials array.
 #pragma once
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 #include "layout.hpp"
 
@@ -67,6 +70,18 @@ __device__ __forceinline__ ChunkView chunk_view(const SideDev& s, int32_t c, int
     cv.sh_vec = window16_shift(cv.d.r0, esize_vec);
     return cv;
 }
+
+// Ops whose gathered vector can be fetched by per-thread async copies expose it as
+// gather_src() and select that policy with gather_l2 == 2 (see the gatherers).
+template <class Op, class = void>
+struct HasGatherSrc : std::false_type {};
+template <class Op>
+struct HasGatherSrc<Op, std::void_t<decltype(std::declval<const Op&>().gather_src())>>
+    : std::true_type {};
+
+template <class Op>
+constexpr bool kAsyncEligible = HasGatherSrc<Op>::value && sizeof(typename Op::MT) == 4 &&
+                                sizeof(typename Op::AT) == 4 && Op::NV == 1;
 
 template <class Op>
 struct TileKernelSmem {
@@ -123,7 +138,9 @@ __device__ __forceinline__ int32_t next_chunk(const SideDev& s, const Op& op, Wo
     }
 }
 
-template <class Op>
+// ASYNC (a separate instantiation, so the register-gather path keeps its own register
+// budget): the gatherers fetch by per-thread async copies; eligible Ops only.
+template <class Op, bool ASYNC = false>
 __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDev s, const Op op) {
     using MT = typename Op::MT;
     using VT = typename Op::VT;
@@ -172,6 +189,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         return;
     }
 
+    constexpr bool async = ASYNC && kAsyncEligible<Op>;
     if (threadIdx.x < NT) {
         // ---- gatherers: products of each chunk, in place over its values ----
         const int g = threadIdx.x;
@@ -196,6 +214,34 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                     float4* v4 = reinterpret_cast<float4*>(buf + cv.lay.off_v);
                     const int32_t quads = (sh0 + K + 3) >> 2;
                     constexpr int QH = 4;  // quads per thread per pass: 16 gathers in flight
+                    if constexpr (async) {
+                        // async policy: each gathered entry is copied (cp.async, 4 bytes)
+                        // over its own column index in the stage, and the products are
+                        // left to the reducers; no register waits on the gathers, whose
+                        // completion arrives on PROD by itself
+                        {
+                            const GT* src = op.gather_src();
+                            const uint32_t ci_base = smem_addr(buf + cv.lay.off_ci);
+                            for (int32_t q0 = g; q0 < quads; q0 += QH * NT) {
+                                int4 cc[QH];
+#pragma unroll
+                                for (int h = 0; h < QH; ++h)
+                                    if (q0 + h * NT < quads) cc[h] = ci4[q0 + h * NT];
+#pragma unroll
+                                for (int h = 0; h < QH; ++h) {
+                                    const int32_t q = q0 + h * NT;
+                                    if (q < quads) {
+                                        const int32_t e = 4 * q - sh0;
+                                        const int cols[4] = {cc[h].x, cc[h].y, cc[h].z, cc[h].w};
+#pragma unroll
+                                        for (int j = 0; j < 4; ++j)
+                                            if (e + j >= 0 && e + j < K)
+                                                cp_async_4(ci_base + 16u * q + 4u * j, src + cols[j]);
+                                    }
+                                }
+                            }
+                        }
+                    } else
                     for (int32_t q0 = g; q0 < quads; q0 += QH * NT) {
                         int4 cc[QH];
                         float4 aa[QH];
@@ -263,9 +309,13 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                     }
                 }
             }
-            mbar_arrive(&sh.prod[st]);  // this thread's products of the stage are in place
+            if (async && c >= 0)
+                cp_async_arrive_noinc(&sh.prod[st]);  // arrives once this thread's copies land
+            else
+                mbar_arrive(&sh.prod[st]);  // this thread's products of the stage are in place
             if (c < 0) break;
         }
+        if constexpr (async) cp_async_wait_all();
         return;
     }
 
@@ -289,6 +339,13 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         const int32_t K = cv.d.k1 - cv.d.k0;
         const AT* p1 = reinterpret_cast<const AT*>(reinterpret_cast<MT*>(buf + cv.lay.off_v) + cv.sh_v);
         const AT* p2 = reinterpret_cast<const AT*>(buf + cv.lay.off_p2);
+        // product k of the first gathered vector: in place over the values, or -- async
+        // policy -- the value times the gathered entry that replaced its column index
+        const AT* g1 = reinterpret_cast<const AT*>(reinterpret_cast<const int32_t*>(buf + cv.lay.off_ci) + cv.sh_ci);
+        auto prod1 = [&](int32_t k) -> AT {
+            if constexpr (async) return mul_rn(p1[k], g1[k]);
+            else return p1[k];
+        };
         const int32_t inst = cv.d.inst;
         if (cv.d.tile != cur_tile) {
             cur_tile = cv.d.tile;
@@ -301,7 +358,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
             // one long row: block reduction over this chunk, accumulated over chunks
             double part[2] = {0.0, 0.0};
             for (int32_t k = r; k < K; k += NT) {
-                part[0] += static_cast<double>(p1[k]);
+                part[0] += static_cast<double>(prod1(k));
                 if (NV > 1) part[1] += static_cast<double>(p2[k]);
             }
             block_sum<NT, 2, kReduceBar>(part, sh.red, r);
@@ -322,7 +379,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                 if (rr < R) {
                     const int32_t e0 = rp_s[rr] - cv.d.k0, e1 = rp_s[rr + 1] - cv.d.k0;
                     for (int32_t k = e0 + lane; k < e1; k += G) {
-                        s1 = add_rn(s1, p1[k]);
+                        s1 = add_rn(s1, prod1(k));
                         if (NV > 1) s2 = add_rn(s2, p2[k]);
                     }
                 }

@@ -122,3 +122,32 @@ def test_one_launch_minor_steps(oracle, examples, name, monkeypatch):
     assert res["0"][0] == res["1"][0]
     assert abs(res["0"][1] - res["1"][1]) <= 0.05 * res["0"][1] + 200
     assert res["1"][2] == pytest.approx(res["0"][2], rel=1e-6, abs=1e-9)
+
+
+@pytest.mark.parametrize("pin", ["12288,128,{p},16384,128,{p},4,3", "24576,128,{p},24576,256,{p},2,4"])
+def test_async_gathers_equal_register_gathers(oracle, monkeypatch, pin):
+    """Gather policy 2 (per-thread async copies into the stage; the reducers form the
+    products) computes every product and sum with the same roundings in the same
+    order as the register gathers: the solves must agree bit for bit, long rows
+    spanning several chunks included."""
+    milp, _ = synthetic.zipf_lp(seed=3, m=4000, n=20000, nnz=300_000)
+    rng = np.random.default_rng(8)
+    I = milp.int_idx
+    xt = np.zeros(len(milp.c))
+    xt[I] = np.round(rng.random(len(I)))
+    monkeypatch.delenv("PDFP_STEP_ENGINE", raising=False)
+    sc, is_eq, is_int, w = oracle.projector_inputs(milp)
+    out = {}
+    for policy in (0, 2):
+        monkeypatch.setenv("PDFP_TUNING", pin.format(p=policy))
+        s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+        tun = (gpu.C.c_int32 * 8)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning(s._h, tun))
+        assert (tun[6], tun[7]) == (policy, policy)
+        s.set_target(xt / sc.D_c)
+        st = s.solve(SolverParameters(eps_optimal_relative=1e-5, eps_feasible_relative=1e-5), 1.0)
+        out[policy] = (st, s.total_count, s.pdhg_x, s.get("pdhg_z"), s.get("current_y"))
+    assert out[0][0] == out[2][0] == "OPTIMAL"
+    assert out[0][1] == out[2][1]
+    for a, b in zip(out[0][2:], out[2][2:]):
+        assert np.array_equal(a, b)
