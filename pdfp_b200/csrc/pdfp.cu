@@ -690,10 +690,8 @@ void Projector::autotune(bool f32) {
         {0, 14 * 1024, 128, 0, 0, 3}, {0, 18 * 1024, 128, 0, 0, 3}, {0, 32 * 1024, 128, 1, 0, 3},
         {1, 0, 0, 0, 2, 4},           {1, 0, 0, 0, 1, 4},           {1, 0, 0, 1, 2, 4},
         // gather policy 2: per-thread async copies into the stage (FP32 steps)
-        {0, 16 * 1024, 128, 2, 0, 3}, {0, 16 * 1024, 128, 2, 0, 4}, {0, 24 * 1024, 128, 2, 0, 3},
-        {0, 24 * 1024, 128, 2, 0, 2}, {0, 32 * 1024, 128, 2, 0, 3}, {0, 32 * 1024, 256, 2, 0, 4},
-        {0, 48 * 1024, 256, 2, 0, 4}, {0, 24 * 1024, 256, 2, 0, 4}, {0, 12 * 1024, 128, 2, 0, 4},
-        {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}};
+        {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}, {0, 24 * 1024, 128, 2, 0, 3},
+        {0, 32 * 1024, 256, 2, 0, 4}};
     constexpr int NC = sizeof(cands) / sizeof(cands[0]);
     cudaEvent_t e0, e1;
     PDFP_CK(cudaEventCreate(&e0));
@@ -863,7 +861,6 @@ void Projector::set_x(int p, const double* x, bool unscaled) {
         load_cols<float>(p, v32_.cx, v32_.ix, unscaled);
     else
         load_cols<double>(p, v64_.cx, v64_.ix, unscaled);
-    PDFP_CK(cudaStreamSynchronize(stream_));
 }
 
 void Projector::set_target(int p, const double* xt, bool unscaled) {
@@ -886,8 +883,7 @@ void Projector::warm_start(int p) {
     else
         launch_elem(K_, len, WarmStartCopy<double>{v64_, M_.col_off, M_.row_off, p}, stream_);
     warm_start_state_kernel<<<1, 1, 0, stream_>>>(st_, p);
-    PDFP_CK(cudaGetLastError());
-    PDFP_CK(cudaStreamSynchronize(stream_));
+    PDFP_CK(cudaGetLastError());  // stream-ordered before the next solve; no host wait
 }
 
 void Projector::get_vector(int p, int which, double* out, bool unscaled) {
@@ -930,6 +926,7 @@ void Projector::get_vector(int p, int which, double* out, bool unscaled) {
 }
 
 void Projector::ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance) {
+    if (sv_ready_) return;  // every instance has its estimate: no state read-back
     std::vector<InstState> hs(K_);
     PDFP_CK(cudaMemcpy(hs.data(), st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost));
     std::vector<int> run(K_, 0);
@@ -938,9 +935,15 @@ void Projector::ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance
         run[p] = (!hs[p].nnz_zero && std::isnan(hs[p].max_sv)) ? 1 : 0;  // cached per run (src/pdfp.jl:225-229)
         any = any || run[p];
     }
-    if (!any) return;
+    if (!any) {
+        sv_ready_ = true;
+        return;
+    }
     std::vector<double> sv = power_iteration(M_, ar_, ev_a_, ev_t_, run, sv_max_iterations,
                                              sv_tolerance, stream_, num_sms_, err_, nullptr);
+    bool all = true;
+    for (int p = 0; p < K_; ++p) all = all && (!run[p] || !std::isnan(sv[p]));
+    sv_ready_ = all;
     DeviceArena tmp;
     double* d = tmp.alloc<double>(K_);
     PDFP_CK(cudaMemcpy(d, sv.data(), sizeof(double) * K_, cudaMemcpyHostToDevice));

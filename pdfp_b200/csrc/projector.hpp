@@ -129,6 +129,7 @@ class Projector {
     } g_;
     std::map<int, cudaGraphExec_t> graphs_;
     bool timing_ = false;
+    bool sv_ready_ = false;  // every instance holds its ||A||_2 estimate
     bool tiny_ = false;  // every member small: a window's minor steps run in one launch
     cudaEvent_t tev_[3] = {nullptr, nullptr, nullptr};     // sampled step kernels (timing mode)
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
