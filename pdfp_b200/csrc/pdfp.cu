@@ -688,6 +688,8 @@ void Projector::autotune(bool f32) {
         {0, 16 * 1024, 128, 1, 0, 3}, {0, 20 * 1024, 128, 1, 0, 3}, {0, 20 * 1024, 128, 0, 0, 3},
         {0, 24 * 1024, 128, 1, 0, 2}, {0, 28 * 1024, 128, 1, 0, 2}, {0, 16 * 1024, 128, 0, 0, 2},
         {0, 14 * 1024, 128, 0, 0, 3}, {0, 18 * 1024, 128, 0, 0, 3}, {0, 32 * 1024, 128, 1, 0, 3},
+        {0, 20 * 1024, 128, 1, 0, 2}, {0, 26 * 1024, 128, 1, 0, 2}, {0, 24 * 1024, 128, 0, 0, 2},
+        {0, 12 * 1024, 128, 1, 0, 4}, {0, 14 * 1024, 128, 1, 0, 3},
         {1, 0, 0, 0, 2, 4},           {1, 0, 0, 0, 1, 4},           {1, 0, 0, 1, 2, 4},
         // gather policy 2: per-thread async copies into the stage (FP32 steps)
         {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}, {0, 24 * 1024, 128, 2, 0, 3},

@@ -244,15 +244,11 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                     } else
                     for (int32_t q0 = g; q0 < quads; q0 += QH * NT) {
                         int4 cc[QH];
-                        float4 aa[QH];
                         GT gv[QH][4][1];
 #pragma unroll
                         for (int h = 0; h < QH; ++h) {
                             const int32_t q = q0 + h * NT;
-                            if (q < quads) {
-                                cc[h] = ci4[q];
-                                aa[h] = v4[q];
-                            }
+                            if (q < quads) cc[h] = ci4[q];
                         }
 #pragma unroll
                         for (int h = 0; h < QH; ++h) {
@@ -269,12 +265,15 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                         for (int h = 0; h < QH; ++h) {
                             const int32_t q = q0 + h * NT;
                             if (q < quads) {
+                                // the values are read only now, after the gathers were
+                                // issued: fewer registers live across their latency
                                 const int32_t e = 4 * q - sh0;
-                                float4 p = aa[h];
-                                if (e + 0 >= 0 && e + 0 < K) p.x = mul_rn(static_cast<float>(aa[h].x), static_cast<float>(gv[h][0][0]));
-                                if (e + 1 >= 0 && e + 1 < K) p.y = mul_rn(static_cast<float>(aa[h].y), static_cast<float>(gv[h][1][0]));
-                                if (e + 2 >= 0 && e + 2 < K) p.z = mul_rn(static_cast<float>(aa[h].z), static_cast<float>(gv[h][2][0]));
-                                if (e + 3 >= 0 && e + 3 < K) p.w = mul_rn(static_cast<float>(aa[h].w), static_cast<float>(gv[h][3][0]));
+                                const float4 a = v4[q];
+                                float4 p = a;
+                                if (e + 0 >= 0 && e + 0 < K) p.x = mul_rn(static_cast<float>(a.x), static_cast<float>(gv[h][0][0]));
+                                if (e + 1 >= 0 && e + 1 < K) p.y = mul_rn(static_cast<float>(a.y), static_cast<float>(gv[h][1][0]));
+                                if (e + 2 >= 0 && e + 2 < K) p.z = mul_rn(static_cast<float>(a.z), static_cast<float>(gv[h][2][0]));
+                                if (e + 3 >= 0 && e + 3 < K) p.w = mul_rn(static_cast<float>(a.w), static_cast<float>(gv[h][3][0]));
                                 v4[q] = p;
                             }
                         }
