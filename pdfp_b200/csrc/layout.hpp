@@ -82,6 +82,7 @@ struct SideDev {
     int32_t rows;
     int32_t n_tiles, n_chunks, max_tile_rows, stage_bytes;
     int32_t stages = 4;  // shared-memory stages per block of the tile engine (2..4)
+    int32_t evict_first = 0;  // tile engine: stream the matrix under an L2 evict-first policy
     const int32_t* rp;
     const int32_t* ci;
     const int32_t* tile_row;     // n_tiles + 1

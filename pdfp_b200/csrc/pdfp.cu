@@ -540,6 +540,9 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     // PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size.
     // PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the step engine (flat1: one quad
     // per thread and tile) and skips the tuner.
+    // PDFP_STREAM_EVICT_FIRST=0 / =1: stream the matrix of the step kernels under
+    // an L2 evict-first policy (off / on)
+    if (const char* ef = std::getenv("PDFP_STREAM_EVICT_FIRST")) evict_first_ = ef[0] == '1';
     const char* at = std::getenv("PDFP_AUTOTUNE");
     const char* se = std::getenv("PDFP_STEP_ENGINE");
     const int forced = !se ? -1
@@ -659,6 +662,7 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     StageGeom g{e, e, e, primal ? 8 : 3, 1, s.stage_bytes, 2048};
     s.tiling = M_.make_tiling(ar_, primal, g);
     s.tiling.dev.stages = s.stages;
+    s.tiling.dev.evict_first = evict_first_ ? 1 : 0;
     const bool async = s.gather_l2 == 2;
     if (primal)
         s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_, async)

@@ -98,7 +98,7 @@ struct TileKernelSmem {
 // Issue the bulk copies of chunk c into stage buffer `buf` (producer lane).
 template <class Op>
 __device__ __forceinline__ void issue_chunk(const SideDev& s, const Op& op, int32_t c,
-                                            unsigned char* buf, uint64_t* bar) {
+                                            unsigned char* buf, uint64_t* bar, uint64_t policy) {
     using MT = typename Op::MT;
     using VT = typename Op::VT;
     using AT = typename Op::AT;
@@ -110,9 +110,17 @@ __device__ __forceinline__ void issue_chunk(const SideDev& s, const Op& op, int3
     const uint32_t b_vec = (cv.last && Op::NVEC > 0) ? window16_bytes(r0, r1, sizeof(VT)) : 0u;
     const uint32_t bytes = b_rp + b_ci + b_v + b_vec * Op::NVEC;
     mbar_arrive_expect_tx(bar, bytes);
-    if (b_rp) bulk_copy_g2s(buf + cv.lay.off_rp, s.rp + (r0 - (int32_t)cv.sh_rp), b_rp, bar);
-    if (b_ci) bulk_copy_g2s(buf + cv.lay.off_ci, s.ci + (k0 - (int32_t)cv.sh_ci), b_ci, bar);
-    if (b_v) bulk_copy_g2s(buf + cv.lay.off_v, op.values() + (k0 - (int32_t)cv.sh_v), b_v, bar);
+    // the matrix streams through once per launch; with s.evict_first its lines leave
+    // L2 first, so the gathered vector and the iterates stay resident
+    if (s.evict_first) {
+        if (b_rp) bulk_copy_g2s_hint(buf + cv.lay.off_rp, s.rp + (r0 - (int32_t)cv.sh_rp), b_rp, bar, policy);
+        if (b_ci) bulk_copy_g2s_hint(buf + cv.lay.off_ci, s.ci + (k0 - (int32_t)cv.sh_ci), b_ci, bar, policy);
+        if (b_v) bulk_copy_g2s_hint(buf + cv.lay.off_v, op.values() + (k0 - (int32_t)cv.sh_v), b_v, bar, policy);
+    } else {
+        if (b_rp) bulk_copy_g2s(buf + cv.lay.off_rp, s.rp + (r0 - (int32_t)cv.sh_rp), b_rp, bar);
+        if (b_ci) bulk_copy_g2s(buf + cv.lay.off_ci, s.ci + (k0 - (int32_t)cv.sh_ci), b_ci, bar);
+        if (b_v) bulk_copy_g2s(buf + cv.lay.off_v, op.values() + (k0 - (int32_t)cv.sh_v), b_v, bar);
+    }
     if (b_vec) {
 #pragma unroll
         for (int k = 0; k < Op::NVEC; ++k)
@@ -167,6 +175,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     if (threadIdx.x >= 2 * NT) {
         // ---- producer: one lane walks the work list and issues the copies ----
         if (threadIdx.x == 2 * NT) {
+            const uint64_t policy = l2_policy_evict_first();
             WorkIter it{-1, 0, 0};
             for (uint32_t u = 0;; ++u) {
                 const int st = u % NS;
@@ -183,7 +192,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                     mbar_arrive(&sh.full[st]);  // completes the phase: the end of the work
                     break;
                 }
-                issue_chunk(s, op, c, dyn_smem + st * (size_t)s.stage_bytes, &sh.full[st]);
+                issue_chunk(s, op, c, dyn_smem + st * (size_t)s.stage_bytes, &sh.full[st], policy);
             }
         }
         return;
