@@ -130,7 +130,7 @@ class Projector {
     std::map<int, cudaGraphExec_t> graphs_;
     bool timing_ = false;
     bool sv_ready_ = false;  // every instance holds its ||A||_2 estimate
-    bool evict_first_ = false;  // step kernels stream the matrix L2 evict-first
+    bool evict_first_ = true;  // step kernels stream the matrix L2 evict-first
     bool tiny_ = false;  // every member small: a window's minor steps run in one launch
     cudaEvent_t tev_[3] = {nullptr, nullptr, nullptr};     // sampled step kernels (timing mode)
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
