@@ -138,6 +138,15 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
 }
 // Block until every cp.async this thread issued has landed (before the thread exits).
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// ---- programmatic dependent launch ------------------------------------------
+// Wait until the grids this one depends on have completed and their writes are
+// visible (returns at once for a grid launched without the programmatic attribute).
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Let the dependent grid be scheduled once every block of this grid has done so
+// (or exited).
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 // Named barrier among the first `nthreads` threads of the block (id 1..15).
 __device__ __forceinline__ void named_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");

@@ -51,15 +51,33 @@ int tile_grid(const SideDev& s, int num_sms, bool async = false) {
     return tile_grid_of<Op, false>(s, num_sms);
 }
 
+template <class Op, bool ASYNC>
+void launch_tile_k(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(2 * Op::NT + 32);
+    cfg.dynamicSmemBytes = tile_dyn_smem<Op>(s);
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = overlap ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, tile_spmv_kernel<Op, ASYNC>, s, op);  // errors: cudaGetLastError
+}
+
+// overlap: the launch may start while the previous grid on the stream drains
+// (programmatic dependent launch; only directly after another tile-engine launch
+// of a step -- see tile_spmv.cuh)
 template <class Op>
-void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream) {
+void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap = false) {
     if (s.n_tiles <= 0 || grid <= 0) return;
     if constexpr (kAsyncEligible<Op>)
         if (op.gather_l2 == 2) {
-            tile_spmv_kernel<Op, true><<<grid, 2 * Op::NT + 32, tile_dyn_smem<Op>(s), stream>>>(s, op);
+            launch_tile_k<Op, true>(s, op, grid, stream, overlap);
             return;
         }
-    tile_spmv_kernel<Op, false><<<grid, 2 * Op::NT + 32, tile_dyn_smem<Op>(s), stream>>>(s, op);
+    launch_tile_k<Op, false>(s, op, grid, stream, overlap);
 }
 
 // ---- launching the flat engine ---------------------------------------------------

@@ -544,6 +544,9 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     // gathered vector and the iterates stay in L2 (zipf-lp: 1% more iterations/s);
     // PDFP_STREAM_EVICT_FIRST=0 / =1 switches it off / on.
     if (const char* ef = std::getenv("PDFP_STREAM_EVICT_FIRST")) evict_first_ = ef[0] == '1';
+    // Consecutive step launches of a window overlap one's drain with the next one's
+    // staging (programmatic dependent launch); PDFP_STEP_OVERLAP=0 / =1 switches it.
+    if (const char* ov = std::getenv("PDFP_STEP_OVERLAP")) overlap_ = ov[0] == '1';
     const char* at = std::getenv("PDFP_AUTOTUNE");
     const char* se = std::getenv("PDFP_STEP_ENGINE");
     const int forced = !se ? -1
@@ -609,25 +612,25 @@ template <>
 IterVecs<double>& Projector::vecs<double>() { return v64_; }
 
 template <typename T, bool MAJOR>
-void Projector::launch_primal(const StepSide& s, int k) {
+void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
     if (s.engine == 1)
         launch_flat(s.tiling.dev, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
     else
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
 }
 
 template <typename T, bool MAJOR>
-void Projector::launch_dual(const StepSide& s, int k) {
+void Projector::launch_dual(const StepSide& s, int k, bool overlap) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
     if (s.engine == 1)
         launch_flat(s.tiling.dev, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
     else
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
 }
 
 // Grid of a step Op family for a tiling (sets the shared-memory attribute of
@@ -972,17 +975,24 @@ void Projector::launch_tiny_steps(int i0, int i1) {
 
 void Projector::record_window(int freq, bool with32, bool with64) {
     const int mode32 = MODE_FP32, mode64 = MODE_FP64;
+    // a step launch directly after another step launch may overlap its drain
+    // (tile engine; see tile_spmv.cuh); after anything else it waits in full
+    bool after_step = false;
+    auto step = [&](auto launch) {
+        launch(overlap_ && after_step);
+        after_step = true;
+    };
     auto prim32 = [&](int k, bool major) {
-        if (major) launch_primal<float, true>(p32_, k); else launch_primal<float, false>(p32_, k);
+        step([&](bool o) { if (major) launch_primal<float, true>(p32_, k, o); else launch_primal<float, false>(p32_, k, o); });
     };
     auto dual32 = [&](int k, bool major) {
-        if (major) launch_dual<float, true>(d32_, k); else launch_dual<float, false>(d32_, k);
+        step([&](bool o) { if (major) launch_dual<float, true>(d32_, k, o); else launch_dual<float, false>(d32_, k, o); });
     };
     auto prim64 = [&](int k, bool major) {
-        if (major) launch_primal<double, true>(p64_, k); else launch_primal<double, false>(p64_, k);
+        step([&](bool o) { if (major) launch_primal<double, true>(p64_, k, o); else launch_primal<double, false>(p64_, k, o); });
     };
     auto dual64 = [&](int k, bool major) {
-        if (major) launch_dual<double, true>(d64_, k); else launch_dual<double, false>(d64_, k);
+        step([&](bool o) { if (major) launch_dual<double, true>(d64_, k, o); else launch_dual<double, false>(d64_, k, o); });
     };
     auto evals = [&](int which) {
         if (with32) {
@@ -1001,21 +1011,26 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             // steps 2 .. freq-1 in one launch per precision
             if (with32) launch_tiny_steps<float>(2, freq);
             if (with64) launch_tiny_steps<double>(2, freq);
+            after_step = false;
             i = freq - 1;
             continue;
         }
         if (sample && i == 2) {
             // events around one minor step of each kernel (timing mode)
+            after_step = false;
             PDFP_CK(cudaEventRecordWithFlags(tev_[0], stream_, cudaEventRecordExternal));
             if (with32) prim32(i, major); else prim64(i, major);
+            after_step = false;
             PDFP_CK(cudaEventRecordWithFlags(tev_[1], stream_, cudaEventRecordExternal));
             if (with32) dual32(i, major); else dual64(i, major);
+            after_step = false;
             PDFP_CK(cudaEventRecordWithFlags(tev_[2], stream_, cudaEventRecordExternal));
             continue;
         }
         if (with32) { prim32(i, major); dual32(i, major); }
         if (with64) { prim64(i, major); dual64(i, major); }
         if (i == 1) {
+            after_step = false;
             evals(EVAL_AFTER_RESTART);
             launch_finalize(K_, Controller{ev_t_.inst_tile0, part_col_, ev_a_.inst_tile0, part_row_, st_, flags_, PHASE_AFTER_FIRST, polish_enabled_}, stream_);
         }

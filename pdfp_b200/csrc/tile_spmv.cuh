@@ -32,6 +32,13 @@
 // are reduced and updated.  The reducers synchronise among themselves with a
 // named barrier; every wait is bounded.
 //
+// Back-to-back step launches may overlap (programmatic dependent launch): the
+// producer reads only data no grid of the chain still writes -- the matrix, the
+// per-row vectors last written two launches back, the instance states -- so it
+// starts staging while the previous grid drains; gatherers and reducers first
+// wait for the previous grid (griddepcontrol.wait), and only then let the next
+// one be scheduled, so a launch never starts before the one two back is done.
+//
 // The Op supplies the types, the gathered vectors, the staged vectors and the
 // per-row epilogue; see pdfp_ops.cuh.  Evaluation Ops also reduce per-tile
 // partial sums (FP64, fixed order) into a partials array.
@@ -202,6 +209,8 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     if (threadIdx.x < NT) {
         // ---- gatherers: products of each chunk, in place over its values ----
         const int g = threadIdx.x;
+        griddep_wait();  // the gathered vector comes from the previous grid
+        griddep_launch_dependents();
         for (uint32_t u = 0;; ++u) {
             const int st = u % NS;
             // Each gatherer waits and arrives on its own: with no barrier among them a
@@ -329,6 +338,8 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
 
     // ---- reducers: row sums and the epilogue ----
     const int r = threadIdx.x - NT;
+    griddep_wait();  // the epilogue writes what the previous grid may still read
+    griddep_launch_dependents();
     double acc[NP > 0 ? NP : 1];
 #pragma unroll
     for (int j = 0; j < (NP > 0 ? NP : 1); ++j) acc[j] = 0.0;

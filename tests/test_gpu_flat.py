@@ -151,3 +151,29 @@ def test_async_gathers_equal_register_gathers(oracle, monkeypatch, pin):
     assert out[0][1] == out[2][1]
     for a, b in zip(out[0][2:], out[2][2:]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_overlapped_step_launches_change_nothing(oracle, monkeypatch, precision):
+    """Consecutive step launches overlap one grid's drain with the next one's staging
+    (programmatic dependent launch); every read of the previous grid's output waits
+    for it, so the solves with and without the overlap agree bit for bit."""
+    milp, _ = synthetic.zipf_lp(seed=5, m=3000, n=12000, nnz=150_000)
+    rng = np.random.default_rng(9)
+    I = milp.int_idx
+    xt = np.zeros(len(milp.c))
+    xt[I] = np.round(rng.random(len(I)))
+    monkeypatch.delenv("PDFP_STEP_ENGINE", raising=False)
+    monkeypatch.setenv("PDFP_AUTOTUNE", "0")
+    sc, is_eq, is_int, w = oracle.projector_inputs(milp)
+    out = {}
+    for ov in ("0", "1"):
+        monkeypatch.setenv("PDFP_STEP_OVERLAP", ov)
+        s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision=precision)
+        s.set_target(xt / sc.D_c)
+        st = s.solve(SolverParameters(eps_optimal_relative=1e-5, eps_feasible_relative=1e-5), 1.0)
+        out[ov] = (st, s.total_count, s.pdhg_x, s.get("pdhg_z"), s.get("current_y"))
+    assert out["0"][0] == out["1"][0] == "OPTIMAL"
+    assert out["0"][1] == out["1"][1]
+    for a, b in zip(out["0"][2:], out["1"][2:]):
+        assert np.array_equal(a, b)
