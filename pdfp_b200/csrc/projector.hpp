@@ -131,7 +131,7 @@ class Projector {
     bool timing_ = false;
     bool sv_ready_ = false;  // every instance holds its ||A||_2 estimate
     bool evict_first_ = true;  // step kernels stream the matrix L2 evict-first
-    bool overlap_ = true;      // consecutive step launches overlap (programmatic launch)
+    bool overlap_ = false;     // consecutive step launches overlap (programmatic launch)
     bool tiny_ = false;  // every member small: a window's minor steps run in one launch
     cudaEvent_t tev_[3] = {nullptr, nullptr, nullptr};     // sampled step kernels (timing mode)
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve

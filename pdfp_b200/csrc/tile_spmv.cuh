@@ -36,8 +36,9 @@
 // producer reads only data no grid of the chain still writes -- the matrix, the
 // per-row vectors last written two launches back, the instance states -- so it
 // starts staging while the previous grid drains; gatherers and reducers first
-// wait for the previous grid (griddepcontrol.wait), and only then let the next
-// one be scheduled, so a launch never starts before the one two back is done.
+// wait for the previous grid (griddepcontrol.wait).  The next grid is let in when
+// every block's producer has staged its last chunk, after a wait of its own, so a
+// launch never starts before the one two back is done.
 //
 // The Op supplies the types, the gathered vectors, the staged vectors and the
 // per-row epilogue; see pdfp_ops.cuh.  Evaluation Ops also reduce per-tile
@@ -197,6 +198,10 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                 sh.stage_chunk[st] = c;
                 if (c < 0) {
                     mbar_arrive(&sh.full[st]);  // completes the phase: the end of the work
+                    // this block has staged all its work: the next grid may be
+                    // scheduled once every block got here (after this grid's own wait)
+                    griddep_wait();
+                    griddep_launch_dependents();
                     break;
                 }
                 issue_chunk(s, op, c, dyn_smem + st * (size_t)s.stage_bytes, &sh.full[st], policy);
@@ -210,7 +215,6 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         // ---- gatherers: products of each chunk, in place over its values ----
         const int g = threadIdx.x;
         griddep_wait();  // the gathered vector comes from the previous grid
-        griddep_launch_dependents();
         for (uint32_t u = 0;; ++u) {
             const int st = u % NS;
             // Each gatherer waits and arrives on its own: with no barrier among them a
@@ -339,7 +343,6 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     // ---- reducers: row sums and the epilogue ----
     const int r = threadIdx.x - NT;
     griddep_wait();  // the epilogue writes what the previous grid may still read
-    griddep_launch_dependents();
     double acc[NP > 0 ? NP : 1];
 #pragma unroll
     for (int j = 0; j < (NP > 0 ? NP : 1); ++j) acc[j] = 0.0;
