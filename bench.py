@@ -246,7 +246,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["zipf-lp", "general-integer", "batch-uneven",
-                                           "pump-markshare"], default="zipf-lp")
+                                           "pump-markshare", "pump-p0201"], default="zipf-lp")
     ap.add_argument("--m", type=int, default=1_000_000)
     ap.add_argument("--n", type=int, default=2_000_000)
     ap.add_argument("--nnz", type=int, default=20_000_000)
@@ -263,8 +263,8 @@ def main():
         return reference_arm(args, world, rank)
     if args.workload == "batch-uneven":
         return batch_uneven(args, world, rank, local)
-    if args.workload == "pump-markshare":
-        return pump_markshare(args, world, rank)
+    if args.workload in PUMP_WORKLOADS:
+        return pump_bench(args, world, rank)
 
     from pdfp_b200 import gpu
     from pdfp_b200.params import SolverParameters
@@ -566,27 +566,43 @@ def batch_uneven(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def pump_markshare(args, world, rank):
-    """Time to first feasible of the pump on 32 markshare-shaped models.
+PUMP_WORKLOADS = {
+    "pump-markshare": ("markshare_like",
+                       "pump-markshare: 6 equality rows x (50 binaries + 6 slacks in [0,1000]), "
+                       "U{0..99} coefficients, b = floor(rowsum/2), model seeds 1..32, pump seeds "
+                       "101 and 201"),
+    "pump-p0201": ("covering_p0201_like",
+                   "pump-p0201: p0201-shaped binary covering, 133 x 201, 1923 nonzeros, "
+                   "coefficients U{1..5}, b = 1 + floor(0.3 rowsum), c U{1..100}, model seeds "
+                   "1..32, pump seeds 101 and 201 (flip_parameter 20, restart_period 100)"),
+}
 
-    Each model: 6 equality knapsack rows over 50 binaries with U{0..99}
-    coefficients plus 6 slacks in [0, 1000] (model seeds 1..32).  Arms: two
+
+def pump_bench(args, world, rank):
+    """Time to first feasible of the pump on 32 small synthetic models.
+
+    pump-markshare: 6 equality knapsack rows over 50 binaries with U{0..99}
+    coefficients plus 6 slacks in [0, 1000].  pump-p0201: binary covering models of
+    p0201's shape (133 x 201, 1923 nonzeros).  Model seeds 1..32.  Arms: two
     trajectories (pump seeds 101 and 201) batched in one projector handle in mixed
     precision; the same two in FP64; and the plain FP64 single-trajectory pump
-    (seed 101).  Reported: p50/p90 of the wall time to the first feasible point,
-    root LP and handle construction included.  Ranks split the model seeds.
+    (seed 101), the drop-in form of the reference's GPU run.  Reported: p50/p90 of
+    the wall time to the first feasible point, root LP and handle construction
+    included.  Ranks split the model seeds.
     """
     from pdfp_b200 import is_feasible, synthetic
     from pdfp_b200.pump import feasibility_pump, feasibility_pump_batched
+    gen_name, config_text = PUMP_WORKLOADS[args.workload]
+    gen = getattr(synthetic, gen_name)
     seeds = [s for s in range(1, 33) if (s - 1) % world == rank]
     arms = {"mixed_batched": [], "fp64_batched": [], "fp64_plain": []}
     found = {k: 0 for k in arms}
-    warm = synthetic.markshare_like(1000)
+    warm = gen(1000)
     for _ in range(args.warmup):
         feasibility_pump_batched(warm, seeds=(101, 201), precision="mixed", time_limit=60)
         feasibility_pump(warm, seed=101, precision="fp64", time_limit=60)
     for s in seeds:
-        m = synthetic.markshare_like(s)
+        m = gen(s)
         t = time.perf_counter()
         r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="mixed", time_limit=60)
         arms["mixed_batched"].append(time.perf_counter() - t)
@@ -616,7 +632,7 @@ def pump_markshare(args, world, rank):
     from oracle import oracle as O
     cpu = []
     for s in range(1, 9):
-        m = synthetic.markshare_like(s)
+        m = gen(s)
         t = time.perf_counter()
         feasibility_pump_batched(m, seeds=(101, 201), solvers=O.OracleSolvers(), time_limit=60)
         cpu.append(time.perf_counter() - t)
@@ -625,9 +641,7 @@ def pump_markshare(args, world, rank):
             "steps": len(arms["mixed_batched"]), "warmup": args.warmup,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": "pump-markshare: 6 equality rows x (50 binaries + 6 slacks in "
-                       "[0,1000]), U{0..99} coefficients, b = floor(rowsum/2), model seeds 1..32, "
-                       "pump seeds 101 and 201"},
+            "config": {"workload": config_text},
             "arms": out,
             "p90_speedup_vs_fp64_plain": round(out["fp64_plain"]["p90_ms"]
                                                / max(out["mixed_batched"]["p90_ms"], 1e-9), 3),
