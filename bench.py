@@ -298,13 +298,18 @@ def main():
                   "a_t_stages": stg[0], "a_stage_bytes": tun[3], "a_threads": tun[4],
                   "a_tiles": tun[5], "a_stages": stg[1], "a_t_gather_l2": tun[6],
                   "a_gather_l2": tun[7]}
+        blk = (gpu.C.c_int32 * 2)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_blocks(st._h, blk))
+        tuning["a_t_blocks_per_sm_cap"] = blk[0]
+        tuning["a_blocks_per_sm_cap"] = blk[1]
         tms = (gpu.C.c_float * 256)()
-        tcfg = (gpu.C.c_int32 * (5 * 256))()
+        tcfg = (gpu.C.c_int32 * (6 * 256))()
         cnt = gpu.C.c_int32()
         gpu.L.check(gpu.L.lib().pdfp_get_tuning_table(st._h, tms, tcfg, 256, gpu.C.byref(cnt)))
         for i in range(min(cnt.value, 256)):
-            log(f"[bench]   tune side={'A' if tcfg[5*i] else 'At'} stage={tcfg[5*i+1]} "
-                f"nt={tcfg[5*i+2]} l2={tcfg[5*i+3]} stages={tcfg[5*i+4]}: {tms[i]*1e3:.1f} us")
+            log(f"[bench]   tune side={'A' if tcfg[6*i] else 'At'} stage={tcfg[6*i+1]} "
+                f"nt={tcfg[6*i+2]} l2={tcfg[6*i+3]} stages={tcfg[6*i+4]} cap={tcfg[6*i+5]}: "
+                f"{tms[i]*1e3:.1f} us")
         log(f"[bench] {precision} handle built in {time.time() - t:.1f}s, tuning {tuning}")
         run_projections(st, warm, x_out, params, False)
         gpu.L.check(gpu.L.lib().pdfp_set_kernel_timing(st._h, 1))
@@ -376,7 +381,7 @@ def main():
                 ("A'z + fused primal/y update", "PrimalOp", tun["a_t_threads"], mx["kp_ms"],
                  bytes_primal32, 252.6e6),
                 ("A x_bar + fused z update", "DualOp", tun["a_threads"], mx["kd_ms"],
-                 bytes_dual32, 188.2e6)]:
+                 bytes_dual32, 187.9e6)]:
             achieved = byts / (ms * 1e-3) / 1e9
             entries.append({"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                             "unit": "GB/s", "frac": round(achieved / peak, 4),

@@ -217,10 +217,11 @@ PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
  * PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size, and
  * PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the engine with its default
  * settings (flat1: the flat engine's one-quad-per-thread variant), and
- * PDFP_TUNING="s,t,l,s,t,l[,n,n]" pins both sides for handles created while it
- * is set: stage bytes, threads per role and the gather policy of A', then of A,
- * with the values out[] below reports, and optionally the stage counts of A'
- * and A (pdfp_get_tuning_stages; default 4).
+ * PDFP_TUNING="s,t,l,s,t,l[,n,n[,b,b]]" pins both sides for handles created
+ * while it is set: stage bytes, threads per role and the gather policy of A',
+ * then of A, with the values out[] below reports, and optionally the stage
+ * counts of A' and A (pdfp_get_tuning_stages; default 4) and their caps on
+ * resident blocks per SM (pdfp_get_tuning_blocks; default 0).
  * out[8] = {A' stage bytes, A' threads per role (0: flat engine), A' tiles,
  * A stage bytes, A threads per role (0: flat engine), A tiles,
  * A' gather policy, A gather policy}. */
@@ -228,10 +229,15 @@ PDFP_API int pdfp_get_tuning(const pdfp_handle* h, int32_t* out);
 /* Shared-memory stages per block of the tile engine on each side: out[2] =
  * {A', A} (2..4; 4 for the flat engine, which has none). */
 PDFP_API int pdfp_get_tuning_stages(const pdfp_handle* h, int32_t* out);
+/* Cap on resident blocks per SM of the tile engine on each side: out[2] = {A', A}
+ * (0: as many as shared memory and registers allow).  With a cap the launch asks
+ * for only those blocks' shared memory, leaving the rest of the SM's unified
+ * L1 / shared memory as L1, where a gather-bound kernel keeps its misses in flight. */
+PDFP_API int pdfp_get_tuning_blocks(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
- * launch time, cfg[5i..5i+4] = {side (0: A', 1: A), stage bytes, threads per
- * role (0: flat engine), gather policy, stages}; *count receives the number
- * of rows. */
+ * launch time, cfg[6i..6i+5] = {side (0: A', 1: A), stage bytes, threads per
+ * role (0: flat engine), gather policy, stages, blocks per SM cap}; *count
+ * receives the number of rows. */
 PDFP_API int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
                                    int32_t* count);
 

@@ -52,32 +52,54 @@ int tile_grid(const SideDev& s, int num_sms, bool async = false) {
 }
 
 template <class Op, bool ASYNC>
-void launch_tile_k(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap) {
+void launch_tile_k(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap,
+                   int carveout) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(grid));
     cfg.blockDim = dim3(2 * Op::NT + 32);
     cfg.dynamicSmemBytes = tile_dyn_smem<Op>(s);
     cfg.stream = stream;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchAttribute at[2];
+    int na = 0;
+    if (overlap) {
+        at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    if (carveout >= 0) {
+        at[na].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+        at[na].val.sharedMemCarveout = static_cast<unsigned>(carveout);
+        ++na;
+    }
     cfg.attrs = at;
-    cfg.numAttrs = overlap ? 1 : 0;
+    cfg.numAttrs = na;
     cudaLaunchKernelEx(&cfg, tile_spmv_kernel<Op, ASYNC>, s, op);  // errors: cudaGetLastError
+}
+
+// Share of the SM's unified L1 / shared memory (percent) that `blocks` resident
+// blocks of this Op need as shared memory on side s: the rest stays L1.
+template <class Op>
+int tile_carveout(const SideDev& s, int blocks, int max_smem_per_sm) {
+    const size_t per_block = tile_dyn_smem<Op>(s) + sizeof(TileKernelSmem<Op>) + 1024;  // + reserved
+    const size_t need = per_block * static_cast<size_t>(blocks);
+    const int pct = static_cast<int>((100 * need + max_smem_per_sm - 1) / max_smem_per_sm);
+    return pct > 100 ? 100 : pct;
 }
 
 // overlap: the launch may start while the previous grid on the stream drains
 // (programmatic dependent launch; only directly after another tile-engine launch
-// of a step -- see tile_spmv.cuh)
+// of a step -- see tile_spmv.cuh).  carveout >= 0: the preferred shared-memory
+// share of the unified L1 (percent) for this launch.
 template <class Op>
-void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap = false) {
+void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap = false,
+                 int carveout = -1) {
     if (s.n_tiles <= 0 || grid <= 0) return;
     if constexpr (kAsyncEligible<Op>)
         if (op.gather_l2 == 2) {
-            launch_tile_k<Op, true>(s, op, grid, stream, overlap);
+            launch_tile_k<Op, true>(s, op, grid, stream, overlap, carveout);
             return;
         }
-    launch_tile_k<Op, false>(s, op, grid, stream, overlap);
+    launch_tile_k<Op, false>(s, op, grid, stream, overlap, carveout);
 }
 
 // ---- launching the flat engine ---------------------------------------------------

@@ -396,6 +396,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     int dev = 0;
     PDFP_CK(cudaGetDevice(&dev));
     PDFP_CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+    PDFP_CK(cudaDeviceGetAttribute(&max_smem_sm_, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     PDFP_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     std::vector<ProblemIn> in;
     for (const ProblemData& p : probs)
@@ -567,13 +568,16 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     // reports them; the tuner does not run.
     bool pinned = false;
     if (const char* pt = std::getenv("PDFP_TUNING")) {
-        int v[8] = {0, 0, 0, 0, 0, 0, 4, 4};
-        const int got = std::sscanf(pt, "%d,%d,%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4],
-                                    &v[5], &v[6], &v[7]);
-        if (got != 6 && got != 8)
-            throw Error(E_INVALID, "PDFP_TUNING must read stage,threads,l2,stage,threads,l2[,stages,stages]");
+        int v[10] = {0, 0, 0, 0, 0, 0, 4, 4, 0, 0};
+        const int got = std::sscanf(pt, "%d,%d,%d,%d,%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3],
+                                    &v[4], &v[5], &v[6], &v[7], &v[8], &v[9]);
+        if (got != 6 && got != 8 && got != 10)
+            throw Error(E_INVALID, "PDFP_TUNING must read stage,threads,l2,stage,threads,l2"
+                                   "[,stages,stages[,blocks,blocks]]");
         if (v[6] < 2 || v[6] > 4 || v[7] < 2 || v[7] > 4)
             throw Error(E_INVALID, "PDFP_TUNING: stages must be 2, 3 or 4");
+        if (v[8] < 0 || v[8] > 8 || v[9] < 0 || v[9] > 8)
+            throw Error(E_INVALID, "PDFP_TUNING: blocks per SM must be 0 (as many as fit) to 8");
         StepSide* sides[2][2] = {{&p32_, &d32_}, {&p64_, &d64_}};
         for (int k = 0; k < 2; ++k)
             for (int f = 0; f < 2; ++f) {
@@ -591,6 +595,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
                 if (c[2] < 0 || c[2] > 2) throw Error(E_INVALID, "PDFP_TUNING: gather policy must be 0, 1 or 2");
                 q.gather_l2 = c[2];
                 q.stages = v[6 + k];
+                q.max_blocks = v[8 + k];
             }
         pinned = true;
     }
@@ -619,9 +624,9 @@ void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
     if (s.engine == 1)
         launch_flat(s.tiling.dev, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
     else
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
 }
 
 template <typename T, bool MAJOR>
@@ -630,9 +635,9 @@ void Projector::launch_dual(const StepSide& s, int k, bool overlap) {
     if (s.engine == 1)
         launch_flat(s.tiling.dev, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
     else
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
 }
 
 // Grid of a step Op family for a tiling (sets the shared-memory attribute of
@@ -676,6 +681,25 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     else
         s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_, async)
                      : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_, async);
+    // A cap on resident blocks per SM: fewer blocks than shared memory allows, with
+    // the unified L1 / shared split asking only for their shared memory, so that
+    // the rest stays L1 (the gathers' in-flight misses live there).
+    s.carveout = -1;
+    if (s.max_blocks > 0 && s.grid > 0) {
+        s.grid = std::min(s.grid, s.max_blocks * num_sms_);
+        const SideDev& d = s.tiling.dev;
+        const int mx = max_smem_sm_;
+        if (s.nt == 256)
+            s.carveout = primal ? (f32 ? tile_carveout<PrimalOp<float, false, 256>>(d, s.max_blocks, mx)
+                                       : tile_carveout<PrimalOp<double, false, 256>>(d, s.max_blocks, mx))
+                                : (f32 ? tile_carveout<DualOp<float, false, 256>>(d, s.max_blocks, mx)
+                                       : tile_carveout<DualOp<double, false, 256>>(d, s.max_blocks, mx));
+        else
+            s.carveout = primal ? (f32 ? tile_carveout<PrimalOp<float, false, 128>>(d, s.max_blocks, mx)
+                                       : tile_carveout<PrimalOp<double, false, 128>>(d, s.max_blocks, mx))
+                                : (f32 ? tile_carveout<DualOp<float, false, 128>>(d, s.max_blocks, mx)
+                                       : tile_carveout<DualOp<double, false, 128>>(d, s.max_blocks, mx));
+    }
 }
 
 // The autotuner: times the minor step kernel of each side for every candidate
@@ -685,6 +709,7 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
 void Projector::autotune(bool f32) {
     struct Cand {
         int engine, stage, nt, l2, qpt, stages;
+        int max_blocks = 0;  // resident blocks per SM (0: as many as fit)
     };
     // tile engine, 4 stages per block: 12-16 KB stages give 3-4 blocks per SM, 24 KB
     // two, 32-48 KB one; 128-thread roles with 2-3 larger stages, 3 blocks per SM;
@@ -701,6 +726,12 @@ void Projector::autotune(bool f32) {
         {0, 20 * 1024, 128, 1, 0, 2}, {0, 26 * 1024, 128, 1, 0, 2}, {0, 24 * 1024, 128, 0, 0, 2},
         {0, 12 * 1024, 128, 1, 0, 4}, {0, 14 * 1024, 128, 1, 0, 3},
         {1, 0, 0, 0, 2, 4},           {1, 0, 0, 0, 1, 4},           {1, 0, 0, 1, 2, 4},
+        // fewer resident blocks than fit, the rest of the unified memory left as L1
+        {0, 24 * 1024, 128, 1, 0, 2, 3}, {0, 20 * 1024, 128, 1, 0, 2, 3}, {0, 16 * 1024, 128, 1, 0, 3, 3},
+        {0, 20 * 1024, 128, 1, 0, 3, 3}, {0, 12 * 1024, 128, 0, 0, 3, 3}, {0, 16 * 1024, 128, 0, 0, 2, 3},
+        {0, 12 * 1024, 128, 0, 0, 4, 3}, {0, 28 * 1024, 128, 1, 0, 2, 2}, {0, 24 * 1024, 128, 1, 0, 3, 2},
+        {0, 16 * 1024, 128, 0, 0, 3, 3}, {0, 22 * 1024, 128, 1, 0, 2, 3}, {0, 26 * 1024, 128, 1, 0, 2, 3},
+        {0, 18 * 1024, 128, 1, 0, 3, 3},
         // gather policy 2: per-thread async copies into the stage (FP32 steps)
         {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}, {0, 24 * 1024, 128, 2, 0, 3},
         {0, 32 * 1024, 256, 2, 0, 4}};
@@ -721,6 +752,7 @@ void Projector::autotune(bool f32) {
             sides[i].stage_bytes = cands[i].stage;
             sides[i].nt = cands[i].nt;
             sides[i].gather_l2 = cands[i].l2;
+            sides[i].max_blocks = cands[i].max_blocks;
             prepare_side(sides[i], primal, f32);
             if (sides[i].grid <= 0) empty_side = true;
         }
@@ -756,7 +788,8 @@ void Projector::autotune(bool f32) {
         }
         int bi = 0;
         for (int i = 0; i < NC; ++i) {
-            tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, cands[i].stages, best_ms[i]});
+            tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, cands[i].stages,
+                                          cands[i].max_blocks, best_ms[i]});
             if (best_ms[i] < best_ms[bi]) bi = i;
         }
         dst = sides[bi];
@@ -778,11 +811,12 @@ int Projector::tuning_table(float* ms, int32_t* cfg, int cap) const {
     const int n = static_cast<int>(tune_table_.size());
     for (int i = 0; i < n && i < cap; ++i) {
         ms[i] = tune_table_[i].ms;
-        cfg[5 * i + 0] = tune_table_[i].side;
-        cfg[5 * i + 1] = tune_table_[i].stage;
-        cfg[5 * i + 2] = tune_table_[i].nt;
-        cfg[5 * i + 3] = tune_table_[i].l2;
-        cfg[5 * i + 4] = tune_table_[i].stages;
+        cfg[6 * i + 0] = tune_table_[i].side;
+        cfg[6 * i + 1] = tune_table_[i].stage;
+        cfg[6 * i + 2] = tune_table_[i].nt;
+        cfg[6 * i + 3] = tune_table_[i].l2;
+        cfg[6 * i + 4] = tune_table_[i].stages;
+        cfg[6 * i + 5] = tune_table_[i].max_blocks;
     }
     return n;
 }
@@ -791,6 +825,12 @@ void Projector::tuning_stages(int32_t* out) const {
     const bool f32 = precision_ == PDFP_MIXED;
     out[0] = (f32 ? p32_ : p64_).stages;
     out[1] = (f32 ? d32_ : d64_).stages;
+}
+
+void Projector::tuning_blocks(int32_t* out) const {
+    const bool f32 = precision_ == PDFP_MIXED;
+    out[0] = (f32 ? p32_ : p64_).max_blocks;
+    out[1] = (f32 ? d32_ : d64_).max_blocks;
 }
 
 void Projector::tuning(int32_t* out) const {

@@ -54,8 +54,10 @@ class Projector {
     // A'-side and the A-side kernel of the handle's base precision.
     void tuning(int32_t* out) const;
     void tuning_stages(int32_t* out) const;
-    // Every autotuner measurement: ms[i] and cfg[4i..4i+3] = {side (0: A', 1: A),
-    // stage bytes, threads per role, gathers cached in L2 only}; returns the count.
+    void tuning_blocks(int32_t* out) const;
+    // Every autotuner measurement: ms[i] and cfg[6i..6i+5] = {side (0: A', 1: A),
+    // stage bytes, threads per role, gather policy, stages, blocks per SM cap};
+    // returns the count.
     int tuning_table(float* ms, int32_t* cfg, int cap) const;
     void set_kernel_timing(bool on) { timing_ = on; }
 
@@ -65,6 +67,8 @@ class Projector {
         int engine = 0;  // 0: tile engine (tile_spmv.cuh), 1: flat engine (flat_spmv.cuh)
         int qpt = 2;     // flat engine: quads (4 nonzeros) per thread and tile, 1 or 2
         int stages = 4;  // tile engine: shared-memory stages per block, 2..4
+        int max_blocks = 0;  // tile engine: resident blocks per SM cap (0: as many as fit)
+        int carveout = -1;   // preferred shared-memory share of L1 for that cap (percent)
         int stage_bytes = 32 * 1024;
         int nt = 256;
         DeviceMatrix::Tiling tiling;
@@ -75,6 +79,7 @@ class Projector {
     struct TuneRow {
         int side, stage, nt, l2;  // nt = 0: the flat engine
         int stages;
+        int max_blocks;
         float ms;
     };
     std::vector<TuneRow> tune_table_;
@@ -100,6 +105,7 @@ class Projector {
     int precision_;
     int K_ = 0;
     int num_sms_ = 148;
+    int max_smem_sm_ = 233472;  // unified L1 / shared memory usable as shared, per SM
     cudaStream_t stream_ = nullptr;
     DeviceArena ar_;
     DeviceMatrix M_;

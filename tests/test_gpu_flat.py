@@ -177,3 +177,31 @@ def test_overlapped_step_launches_change_nothing(oracle, monkeypatch, precision)
     assert out["0"][1] == out["1"][1]
     for a, b in zip(out["0"][2:], out["1"][2:]):
         assert np.array_equal(a, b)
+
+
+def test_blocks_per_sm_cap_changes_nothing(oracle, monkeypatch):
+    """A cap on resident blocks per SM (with the launch's shared-memory carveout
+    sized for it) changes only where the tiles run: the same solve bit for bit."""
+    milp, _ = synthetic.zipf_lp(seed=3, m=4000, n=20000, nnz=300_000)
+    rng = np.random.default_rng(8)
+    I = milp.int_idx
+    xt = np.zeros(len(milp.c))
+    xt[I] = np.round(rng.random(len(I)))
+    monkeypatch.delenv("PDFP_STEP_ENGINE", raising=False)
+    sc, is_eq, is_int, w = oracle.projector_inputs(milp)
+    out = {}
+    for cap in (0, 2):
+        monkeypatch.setenv("PDFP_TUNING", f"12288,128,0,24576,128,1,3,2,{cap},{cap}")
+        s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+        blk = (gpu.C.c_int32 * 2)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_blocks(s._h, blk))
+        assert list(blk) == [cap, cap]
+        s.set_target(xt / sc.D_c)
+        st = s.solve(SolverParameters(eps_optimal_relative=1e-5, eps_feasible_relative=1e-5), 1.0)
+        out[cap] = (st, s.total_count, s.pdhg_x, s.get("pdhg_z"))
+    assert out[0][0] == out[2][0] == "OPTIMAL" and out[0][1] == out[2][1]
+    for a, b in zip(out[0][2:], out[2][2:]):
+        assert np.array_equal(a, b)
+    monkeypatch.setenv("PDFP_TUNING", "12288,128,0,24576,128,1,3,2,9,0")
+    with pytest.raises(Exception, match="blocks per SM"):
+        gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
