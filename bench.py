@@ -302,14 +302,18 @@ def main():
         gpu.L.check(gpu.L.lib().pdfp_get_tuning_blocks(st._h, blk))
         tuning["a_t_blocks_per_sm_cap"] = blk[0]
         tuning["a_blocks_per_sm_cap"] = blk[1]
+        red = (gpu.C.c_int32 * 2)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_reducers(st._h, red))
+        tuning["a_t_reducers"] = red[0]
+        tuning["a_reducers"] = red[1]
         tms = (gpu.C.c_float * 256)()
-        tcfg = (gpu.C.c_int32 * (6 * 256))()
+        tcfg = (gpu.C.c_int32 * (7 * 256))()
         cnt = gpu.C.c_int32()
         gpu.L.check(gpu.L.lib().pdfp_get_tuning_table(st._h, tms, tcfg, 256, gpu.C.byref(cnt)))
         for i in range(min(cnt.value, 256)):
-            log(f"[bench]   tune side={'A' if tcfg[6*i] else 'At'} stage={tcfg[6*i+1]} "
-                f"nt={tcfg[6*i+2]} l2={tcfg[6*i+3]} stages={tcfg[6*i+4]} cap={tcfg[6*i+5]}: "
-                f"{tms[i]*1e3:.1f} us")
+            log(f"[bench]   tune side={'A' if tcfg[7*i] else 'At'} stage={tcfg[7*i+1]} "
+                f"nt={tcfg[7*i+2]} l2={tcfg[7*i+3]} stages={tcfg[7*i+4]} cap={tcfg[7*i+5]} "
+                f"red={tcfg[7*i+6]}: {tms[i]*1e3:.1f} us")
         log(f"[bench] {precision} handle built in {time.time() - t:.1f}s, tuning {tuning}")
         run_projections(st, warm, x_out, params, False)
         gpu.L.check(gpu.L.lib().pdfp_set_kernel_timing(st._h, 1))

@@ -220,8 +220,9 @@ PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
  * PDFP_TUNING="s,t,l,s,t,l[,n,n[,b,b]]" pins both sides for handles created
  * while it is set: stage bytes, threads per role and the gather policy of A',
  * then of A, with the values out[] below reports, and optionally the stage
- * counts of A' and A (pdfp_get_tuning_stages; default 4) and their caps on
- * resident blocks per SM (pdfp_get_tuning_blocks; default 0).
+ * counts of A' and A (pdfp_get_tuning_stages; default 4), their caps on
+ * resident blocks per SM (pdfp_get_tuning_blocks; default 0) and their reducer
+ * threads (pdfp_get_tuning_reducers; 0: as many as gatherers).
  * out[8] = {A' stage bytes, A' threads per role (0: flat engine), A' tiles,
  * A stage bytes, A threads per role (0: flat engine), A tiles,
  * A' gather policy, A gather policy}. */
@@ -234,10 +235,14 @@ PDFP_API int pdfp_get_tuning_stages(const pdfp_handle* h, int32_t* out);
  * for only those blocks' shared memory, leaving the rest of the SM's unified
  * L1 / shared memory as L1, where a gather-bound kernel keeps its misses in flight. */
 PDFP_API int pdfp_get_tuning_blocks(const pdfp_handle* h, int32_t* out);
+/* Reducer threads per block of the tile engine on each side: out[2] = {A', A}
+ * (the gatherers are the threads per role of pdfp_get_tuning; FP32 steps may run
+ * half as many reducers as gatherers; 0 for the flat engine). */
+PDFP_API int pdfp_get_tuning_reducers(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
- * launch time, cfg[6i..6i+5] = {side (0: A', 1: A), stage bytes, threads per
- * role (0: flat engine), gather policy, stages, blocks per SM cap}; *count
- * receives the number of rows. */
+ * launch time, cfg[7i..7i+6] = {side (0: A', 1: A), stage bytes, gatherer
+ * threads (0: flat engine), gather policy, stages, blocks per SM cap, reducer
+ * threads}; *count receives the number of rows. */
 PDFP_API int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
                                    int32_t* count);
 

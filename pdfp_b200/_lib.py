@@ -113,6 +113,7 @@ SIGNATURES = {
     "pdfp_get_tuning_table": (C.c_int, [vp, C.POINTER(C.c_float), ip, C.c_int32, ip]),
     "pdfp_get_tuning_stages": (C.c_int, [vp, ip]),
     "pdfp_get_tuning_blocks": (C.c_int, [vp, ip]),
+    "pdfp_get_tuning_reducers": (C.c_int, [vp, ip]),
     "pdfp_profile_step": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                     dp, dp]),
     "pdfp_scale_problem": (C.c_int, [C.POINTER(Csr), dp, dp, dp, dp, dp, C.c_int32, C.c_double,

@@ -568,12 +568,12 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     // reports them; the tuner does not run.
     bool pinned = false;
     if (const char* pt = std::getenv("PDFP_TUNING")) {
-        int v[10] = {0, 0, 0, 0, 0, 0, 4, 4, 0, 0};
-        const int got = std::sscanf(pt, "%d,%d,%d,%d,%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3],
-                                    &v[4], &v[5], &v[6], &v[7], &v[8], &v[9]);
-        if (got != 6 && got != 8 && got != 10)
+        int v[12] = {0, 0, 0, 0, 0, 0, 4, 4, 0, 0, 0, 0};
+        const int got = std::sscanf(pt, "%d,%d,%d,%d,%d,%d,%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2],
+                                    &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &v[11]);
+        if (got != 6 && got != 8 && got != 10 && got != 12)
             throw Error(E_INVALID, "PDFP_TUNING must read stage,threads,l2,stage,threads,l2"
-                                   "[,stages,stages[,blocks,blocks]]");
+                                   "[,stages,stages[,blocks,blocks[,reducers,reducers]]]");
         if (v[6] < 2 || v[6] > 4 || v[7] < 2 || v[7] > 4)
             throw Error(E_INVALID, "PDFP_TUNING: stages must be 2, 3 or 4");
         if (v[8] < 0 || v[8] > 8 || v[9] < 0 || v[9] > 8)
@@ -596,6 +596,11 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
                 q.gather_l2 = c[2];
                 q.stages = v[6 + k];
                 q.max_blocks = v[8 + k];
+                const int red = v[10 + k];
+                if (red != 0 && red != c[1] && !(c[1] != 0 && red == c[1] / 2))
+                    throw Error(E_INVALID, "PDFP_TUNING: reducers must be 0, the threads per role "
+                                           "or half of them");
+                q.half_red = c[1] != 0 && red == c[1] / 2;
             }
         pinned = true;
     }
@@ -624,9 +629,9 @@ void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
     if (s.engine == 1)
         launch_flat(s.tiling.dev, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
     else
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
 }
 
 template <typename T, bool MAJOR>
@@ -635,21 +640,21 @@ void Projector::launch_dual(const StepSide& s, int k, bool overlap) {
     if (s.engine == 1)
         launch_flat(s.tiling.dev, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
     else
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
 }
 
 // Grid of a step Op family for a tiling (sets the shared-memory attribute of
 // both the MAJOR and the minor kernel).
 template <template <typename, bool, int> class OpT, typename T>
-static int step_grid(const SideDev& d, int nt, int sms, bool async) {
+static int step_grid(const SideDev& d, int nt, int sms, bool async, bool half_red) {
     if (nt == 256) {
-        tile_grid<OpT<T, false, 256>>(d, sms, async);
-        return tile_grid<OpT<T, true, 256>>(d, sms, async);
+        tile_grid<OpT<T, false, 256>>(d, sms, async, half_red);
+        return tile_grid<OpT<T, true, 256>>(d, sms, async, half_red);
     }
-    tile_grid<OpT<T, false, 128>>(d, sms, async);
-    return tile_grid<OpT<T, true, 128>>(d, sms, async);
+    tile_grid<OpT<T, false, 128>>(d, sms, async, half_red);
+    return tile_grid<OpT<T, true, 128>>(d, sms, async, half_red);
 }
 
 void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
@@ -675,12 +680,13 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     s.tiling.dev.stages = s.stages;
     s.tiling.dev.evict_first = evict_first_ ? 1 : 0;
     const bool async = s.gather_l2 == 2;
+    if (!f32 || async) s.half_red = false;  // half-size reducers: FP32 register-gather steps only
     if (primal)
-        s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_, async)
-                     : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_, async);
+        s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_, async, s.half_red)
+                     : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_, async, false);
     else
-        s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_, async)
-                     : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_, async);
+        s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_, async, s.half_red)
+                     : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_, async, false);
     // A cap on resident blocks per SM: fewer blocks than shared memory allows, with
     // the unified L1 / shared split asking only for their shared memory, so that
     // the rest stays L1 (the gathers' in-flight misses live there).
@@ -710,6 +716,7 @@ void Projector::autotune(bool f32) {
     struct Cand {
         int engine, stage, nt, l2, qpt, stages;
         int max_blocks = 0;  // resident blocks per SM (0: as many as fit)
+        int half_red = 0;    // 1: nt / 2 reducer threads
     };
     // tile engine, 4 stages per block: 12-16 KB stages give 3-4 blocks per SM, 24 KB
     // two, 32-48 KB one; 128-thread roles with 2-3 larger stages, 3 blocks per SM;
@@ -732,6 +739,8 @@ void Projector::autotune(bool f32) {
         {0, 12 * 1024, 128, 0, 0, 4, 3}, {0, 28 * 1024, 128, 1, 0, 2, 2}, {0, 24 * 1024, 128, 1, 0, 3, 2},
         {0, 16 * 1024, 128, 0, 0, 3, 3}, {0, 22 * 1024, 128, 1, 0, 2, 3}, {0, 26 * 1024, 128, 1, 0, 2, 3},
         {0, 18 * 1024, 128, 1, 0, 3, 3},
+        // 256 gatherers with 128 reducers
+        {0, 24 * 1024, 256, 0, 0, 2, 0, 1}, {0, 32 * 1024, 256, 1, 0, 2, 0, 1},
         // gather policy 2: per-thread async copies into the stage (FP32 steps)
         {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}, {0, 24 * 1024, 128, 2, 0, 3},
         {0, 32 * 1024, 256, 2, 0, 4}};
@@ -753,6 +762,7 @@ void Projector::autotune(bool f32) {
             sides[i].nt = cands[i].nt;
             sides[i].gather_l2 = cands[i].l2;
             sides[i].max_blocks = cands[i].max_blocks;
+            sides[i].half_red = cands[i].half_red != 0;
             prepare_side(sides[i], primal, f32);
             if (sides[i].grid <= 0) empty_side = true;
         }
@@ -789,7 +799,8 @@ void Projector::autotune(bool f32) {
         int bi = 0;
         for (int i = 0; i < NC; ++i) {
             tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, cands[i].stages,
-                                          cands[i].max_blocks, best_ms[i]});
+                                          cands[i].max_blocks,
+                                          sides[i].half_red ? cands[i].nt / 2 : cands[i].nt, best_ms[i]});
             if (best_ms[i] < best_ms[bi]) bi = i;
         }
         dst = sides[bi];
@@ -811,12 +822,13 @@ int Projector::tuning_table(float* ms, int32_t* cfg, int cap) const {
     const int n = static_cast<int>(tune_table_.size());
     for (int i = 0; i < n && i < cap; ++i) {
         ms[i] = tune_table_[i].ms;
-        cfg[6 * i + 0] = tune_table_[i].side;
-        cfg[6 * i + 1] = tune_table_[i].stage;
-        cfg[6 * i + 2] = tune_table_[i].nt;
-        cfg[6 * i + 3] = tune_table_[i].l2;
-        cfg[6 * i + 4] = tune_table_[i].stages;
-        cfg[6 * i + 5] = tune_table_[i].max_blocks;
+        cfg[7 * i + 0] = tune_table_[i].side;
+        cfg[7 * i + 1] = tune_table_[i].stage;
+        cfg[7 * i + 2] = tune_table_[i].nt;
+        cfg[7 * i + 3] = tune_table_[i].l2;
+        cfg[7 * i + 4] = tune_table_[i].stages;
+        cfg[7 * i + 5] = tune_table_[i].max_blocks;
+        cfg[7 * i + 6] = tune_table_[i].reducers;
     }
     return n;
 }
@@ -831,6 +843,14 @@ void Projector::tuning_blocks(int32_t* out) const {
     const bool f32 = precision_ == PDFP_MIXED;
     out[0] = (f32 ? p32_ : p64_).max_blocks;
     out[1] = (f32 ? d32_ : d64_).max_blocks;
+}
+
+void Projector::tuning_reducers(int32_t* out) const {
+    const bool f32 = precision_ == PDFP_MIXED;
+    const StepSide& p = f32 ? p32_ : p64_;
+    const StepSide& d = f32 ? d32_ : d64_;
+    out[0] = p.engine == 1 ? 0 : (p.half_red ? p.nt / 2 : p.nt);
+    out[1] = d.engine == 1 ? 0 : (d.half_red ? d.nt / 2 : d.nt);
 }
 
 void Projector::tuning(int32_t* out) const {

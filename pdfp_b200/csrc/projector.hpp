@@ -55,9 +55,10 @@ class Projector {
     void tuning(int32_t* out) const;
     void tuning_stages(int32_t* out) const;
     void tuning_blocks(int32_t* out) const;
-    // Every autotuner measurement: ms[i] and cfg[6i..6i+5] = {side (0: A', 1: A),
-    // stage bytes, threads per role, gather policy, stages, blocks per SM cap};
-    // returns the count.
+    void tuning_reducers(int32_t* out) const;
+    // Every autotuner measurement: ms[i] and cfg[7i..7i+6] = {side (0: A', 1: A),
+    // stage bytes, gatherer threads, gather policy, stages, blocks per SM cap,
+    // reducer threads}; returns the count.
     int tuning_table(float* ms, int32_t* cfg, int cap) const;
     void set_kernel_timing(bool on) { timing_ = on; }
 
@@ -69,6 +70,7 @@ class Projector {
         int stages = 4;  // tile engine: shared-memory stages per block, 2..4
         int max_blocks = 0;  // tile engine: resident blocks per SM cap (0: as many as fit)
         int carveout = -1;   // preferred shared-memory share of L1 for that cap (percent)
+        bool half_red = false;  // tile engine: nt / 2 reducer threads (FP32 steps)
         int stage_bytes = 32 * 1024;
         int nt = 256;
         DeviceMatrix::Tiling tiling;
@@ -80,6 +82,7 @@ class Projector {
         int side, stage, nt, l2;  // nt = 0: the flat engine
         int stages;
         int max_blocks;
+        int reducers;
         float ms;
     };
     std::vector<TuneRow> tune_table_;

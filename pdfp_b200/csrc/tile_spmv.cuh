@@ -20,9 +20,10 @@
 //             completes when all NT have).  No barrier joins them, so threads
 //             drift up to kStages stages apart and gathers of several stages
 //             overlap.
-//   REDUCERS  (NT threads) wait on PROD, sum each row in shared memory (G lanes
-//             per row; G = 1 sums a row sequentially in ascending storage order,
-//             which is the reference's order; a long row uses a block
+//   REDUCERS  (NRED threads: NT, or NT / 2 for FP32 steps) wait on PROD, sum
+//             each row in shared memory (G lanes per row; G = 1 sums a row
+//             sequentially in ascending storage order, which is the
+//             reference's order; a long row uses a block
 //             reduction accumulated over its chunks) and, on a tile's last
 //             chunk, run the epilogue -- one thread per row, consecutive rows on
 //             consecutive threads: the fused PDHG update (or an evaluation
@@ -100,7 +101,7 @@ struct TileKernelSmem {
     int32_t stage_chunk[kStages];
     int32_t flag;
     typename Op::AT long_acc[Op::NV > 0 ? Op::NV : 1];
-    double red[(NP > 2 ? NP : 2) * (Op::NT / 32)];
+    double red[(NP > 2 ? NP : 2) * (Op::NT / 32)];  // sized for up to Op::NT reducers
 };
 
 // Issue the bulk copies of chunk c into stage buffer `buf` (producer lane).
@@ -156,13 +157,16 @@ __device__ __forceinline__ int32_t next_chunk(const SideDev& s, const Op& op, Wo
 
 // ASYNC (a separate instantiation, so the register-gather path keeps its own register
 // budget): the gatherers fetch by per-thread async copies; eligible Ops only.
-template <class Op, bool ASYNC = false>
-__global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDev s, const Op op) {
+// NRED: reducer threads (a multiple of 32, at most Op::NT); the gatherers are Op::NT.
+template <class Op, bool ASYNC = false, int NRED = Op::NT>
+__global__ void __launch_bounds__(Op::NT + NRED + 32) tile_spmv_kernel(const SideDev s, const Op op) {
     using MT = typename Op::MT;
     using VT = typename Op::VT;
     using AT = typename Op::AT;
     using GT = typename Op::GT;
     constexpr int NT = Op::NT, NV = Op::NV, NVEC = Op::NVEC, NP = Op::NP;
+    constexpr int NR = NRED;
+    static_assert(NR % 32 == 0 && NR <= NT, "reducers: a multiple of 32, at most the gatherers");
     constexpr int UNROLL = sizeof(MT) == 4 ? 16 : 8;  // scalar path: gathers in flight per thread
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     __shared__ TileKernelSmem<Op> sh;
@@ -180,9 +184,9 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
     }
     __syncthreads();
 
-    if (threadIdx.x >= 2 * NT) {
+    if (threadIdx.x >= NT + NR) {
         // ---- producer: one lane walks the work list and issues the copies ----
-        if (threadIdx.x == 2 * NT) {
+        if (threadIdx.x == NT + NR) {
             const uint64_t policy = l2_policy_evict_first();
             WorkIter it{-1, 0, 0};
             for (uint32_t u = 0;; ++u) {
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
 
     for (uint32_t u = 0;; ++u) {
         const int st = u % NS;
-        if (!group_wait(&sh.prod[st], (u / NS) & 1u, op.err(), r == 0, kReduceBar, NT, &sh.flag))
+        if (!group_wait(&sh.prod[st], (u / NS) & 1u, op.err(), r == 0, kReduceBar, NR, &sh.flag))
             break;  // a wait gave up (error recorded)
         const int32_t c = sh.stage_chunk[st];
         if (c < 0) break;
@@ -379,11 +383,11 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         if (cv.single) {
             // one long row: block reduction over this chunk, accumulated over chunks
             double part[2] = {0.0, 0.0};
-            for (int32_t k = r; k < K; k += NT) {
+            for (int32_t k = r; k < K; k += NR) {
                 part[0] += static_cast<double>(prod1(k));
                 if (NV > 1) part[1] += static_cast<double>(p2[k]);
             }
-            block_sum<NT, 2, kReduceBar>(part, sh.red, r);
+            block_sum<NR, 2, kReduceBar>(part, sh.red, r);
             if (r == 0) {
                 const bool first = cv.d.first != 0;
                 sh.long_acc[0] = (first ? AT(0) : sh.long_acc[0]) + static_cast<AT>(part[0]);
@@ -392,8 +396,8 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
         } else if (NV > 0) {
             const int32_t* rp_s = reinterpret_cast<const int32_t*>(buf + cv.lay.off_rp) + cv.sh_rp;
             int G = 1;
-            while (G < 32 && G * 2 * R <= NT) G *= 2;
-            const int groups = NT / G;
+            while (G < 32 && G * 2 * R <= NR) G *= 2;
+            const int groups = NR / G;
             const int gid = r / G, lane = r & (G - 1);
             for (int32_t base = 0; base < R; base += groups) {
                 const int32_t rr = base + gid;
@@ -418,12 +422,12 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
 
         // epilogue on the tile's last chunk
         if (cv.last) {
-            named_sync(kReduceBar, NT);
+            named_sync(kReduceBar, NR);
             const VT* sv[NVEC > 0 ? NVEC : 1];
 #pragma unroll
             for (int k = 0; k < NVEC; ++k)
                 sv[k] = reinterpret_cast<const VT*>(buf + cv.lay.off_vec0 + k * cv.lay.vec_stride) + cv.sh_vec;
-            for (int32_t rr = r; rr < R; rr += NT) {
+            for (int32_t rr = r; rr < R; rr += NR) {
                 AT sums[NV > 0 ? NV : 1];
                 if (cv.single) {
 #pragma unroll
@@ -435,13 +439,13 @@ __global__ void __launch_bounds__(2 * Op::NT + 32) tile_spmv_kernel(const SideDe
                 op.row(cv.d.r0 + rr, rr, inst, tp, sv, sums, acc);
             }
             if constexpr (NP > 0) {
-                block_sum<NT, NP, kReduceBar>(acc, sh.red, r);
+                block_sum<NR, NP, kReduceBar>(acc, sh.red, r);
                 if (r == 0) op.write_partials(cv.d.tile, acc);
 #pragma unroll
                 for (int j = 0; j < NP; ++j) acc[j] = 0.0;
             }
         }
-        named_sync(kReduceBar, NT);  // stage `st` fully consumed
+        named_sync(kReduceBar, NR);  // stage `st` fully consumed
         if (r == 0) {
             fence_proxy_async_smem();  // generic-proxy writes (products) before the next bulk copy
             mbar_arrive(&sh.empty[st]);

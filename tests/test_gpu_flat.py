@@ -205,3 +205,34 @@ def test_blocks_per_sm_cap_changes_nothing(oracle, monkeypatch):
     monkeypatch.setenv("PDFP_TUNING", "12288,128,0,24576,128,1,3,2,9,0")
     with pytest.raises(Exception, match="blocks per SM"):
         gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+
+
+def test_half_size_reducer_role_agrees(oracle, monkeypatch):
+    """256 gatherers with 128 reducers: the row sums group lanes by the reducer count,
+    so roundings may differ from the 256/256 kernel; the projection agrees within the
+    mixed-form tolerances (same status, iteration counts within 5%, l1 distances within
+    1e-3 relative), long rows spanning several chunks included."""
+    milp, _ = synthetic.zipf_lp(seed=3, m=4000, n=20000, nnz=300_000)
+    rng = np.random.default_rng(8)
+    I = milp.int_idx
+    xt = np.zeros(len(milp.c))
+    xt[I] = np.round(rng.random(len(I)))
+    monkeypatch.delenv("PDFP_STEP_ENGINE", raising=False)
+    sc, is_eq, is_int, w = oracle.projector_inputs(milp)
+    res = {}
+    for red in (256, 128):
+        monkeypatch.setenv("PDFP_TUNING", f"16384,256,0,24576,256,1,3,2,0,0,{red},{red}")
+        s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+        r = (gpu.C.c_int32 * 2)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_reducers(s._h, r))
+        assert list(r) == [red, red]
+        s.set_target(xt / sc.D_c)
+        st = s.solve(SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-4), 1.0)
+        x = sc.D_c * s.pdhg_x
+        res[red] = (st, s.total_count, float(np.sum(w[I] * np.abs(x[I] - xt[I]) / sc.D_c[I])))
+    assert res[256][0] == res[128][0] == "OPTIMAL"
+    assert abs(res[256][1] - res[128][1]) <= 0.05 * res[256][1] + 64
+    assert res[128][2] == pytest.approx(res[256][2], rel=1e-3)
+    monkeypatch.setenv("PDFP_TUNING", "16384,256,0,24576,256,1,3,2,0,0,96,0")
+    with pytest.raises(Exception, match="reducers"):
+        gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
