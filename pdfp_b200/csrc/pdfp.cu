@@ -452,6 +452,8 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     sp_ = ar_.alloc<SolveParams>(K_);
     stage_ = ar_.alloc<double>(std::max<int64_t>(std::max(M_.max_m, M_.max_n), 1));
     PDFP_CK(cudaMallocHost(&flags_h_, sizeof(InstFlags) * (K_ + 1)));
+    PDFP_CK(cudaMallocHost(&st_h_, sizeof(InstState) * K_));
+    host_total_.assign(K_, 0);
     PDFP_CK(cudaMallocHost(&nan_seen_h_, sizeof(int32_t)));
     vec_mode_.assign(K_, precision_ == PDFP_MIXED ? MODE_FP32 : MODE_FP64);
 
@@ -873,6 +875,7 @@ Projector::~Projector() {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     graphs_.clear();
     if (flags_h_) cudaFreeHost(flags_h_);
+    if (st_h_) cudaFreeHost(st_h_);
     if (nan_seen_h_) cudaFreeHost(nan_seen_h_);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -955,6 +958,7 @@ void Projector::warm_start(int p) {
     else
         launch_elem(K_, len, WarmStartCopy<double>{v64_, M_.col_off, M_.row_off, p}, stream_);
     warm_start_state_kernel<<<1, 1, 0, stream_>>>(st_, p);
+    host_total_[p] = 0;
     PDFP_CK(cudaGetLastError());  // stream-ordered before the next solve; no host wait
 }
 
@@ -1195,9 +1199,18 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     PDFP_CK(cudaGetLastError());
     PDFP_CK(cudaMemsetAsync(err_, 0, sizeof(int32_t) * 4, stream_));
 
-    // first poll: instances may already be done (iteration_limit <= total)
-    PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
-    PDFP_CK(cudaStreamSynchronize(stream_));
+    // Which instances start running (iteration_limit > total): solve_init_kernel's
+    // rule, evaluated on the host from the totals it tracks, so that no first poll
+    // is needed; after a call that advanced the state otherwise, read it back.
+    if (totals_known_) {
+        for (int p = 0; p < K_; ++p)
+            flags_h_[p] = InstFlags{host_total_[p] < sp[p].iter_limit ? ST_RUNNING : ST_ITERATION_LIMIT,
+                                    sp[p].mode, 0, 0};
+    } else {
+        PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
+        PDFP_CK(cudaStreamSynchronize(stream_));
+    }
+    bool polled = false;  // st_h_ holds the state after the last window
     int32_t dev_err = 0;
     double kp_sum = 0.0, kd_sum = 0.0;
     int64_t k_samples = 0;
@@ -1209,7 +1222,12 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         PDFP_CK(cudaGraphLaunch(g, stream_));
         PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
         PDFP_CK(cudaMemcpyAsync(&flags_h_[K_].status, err_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+        // the states too, and the end event: the poll that finds every instance
+        // done then needs no further round trip
+        PDFP_CK(cudaMemcpyAsync(st_h_, st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost, stream_));
+        PDFP_CK(cudaEventRecord(sev_[1], stream_));
         PDFP_CK(cudaStreamSynchronize(stream_));
+        polled = true;
         dev_err = flags_h_[K_].status;
         if (dev_err) throw Error(E_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
         if (timing_ && freq >= 3 && (with32 != with64)) {
@@ -1231,15 +1249,18 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
                 vec_mode_[p] = MODE_FP64;
                 with64 = true;
                 polished_.insert(p);
+                polled = false;
             }
         }
         const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
         if (wall > max_time + 120.0) throw Error(E_TIMEOUT, "solve exceeded its time limit by 120 s on the host clock");
     }
-    PDFP_CK(cudaEventRecord(sev_[1], stream_));
-    std::vector<InstState> hs(K_);
-    PDFP_CK(cudaMemcpyAsync(hs.data(), st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost, stream_));
-    PDFP_CK(cudaStreamSynchronize(stream_));
+    if (!polled) {
+        PDFP_CK(cudaMemcpyAsync(st_h_, st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost, stream_));
+        PDFP_CK(cudaEventRecord(sev_[1], stream_));
+        PDFP_CK(cudaStreamSynchronize(stream_));
+    }
+    const InstState* hs = st_h_;
     float solve_ms = 0.f;
     PDFP_CK(cudaEventElapsedTime(&solve_ms, sev_[0], sev_[1]));
     for (int p = 0; p < K_; ++p) {
@@ -1264,12 +1285,15 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         r.kernel_ms_dual = k_samples ? kd_sum / k_samples : 0.0;
         r.kernel_samples = k_samples;
         vec_mode_[p] = s.mode;
+        host_total_[p] = s.total;
     }
+    totals_known_ = true;
     polished_.clear();
 }
 
 void Projector::profile_step(int iterations, float* ms_primal, float* ms_dual, double* bytes_primal,
                              double* bytes_dual) {
+    totals_known_ = false;  // the next solve reads the instance states back first
     // Times the two fused step kernels (minor steps) over `iterations` steps of
     // every running instance, with events around each launch on the stream.
     const bool mixed = precision_ == PDFP_MIXED;

@@ -122,6 +122,9 @@ class Projector {
     InstState* st_ = nullptr;
     InstFlags* flags_ = nullptr;
     InstFlags* flags_h_ = nullptr;
+    InstState* st_h_ = nullptr;       // page-locked copy of the states, read with each poll
+    std::vector<int64_t> host_total_;  // PDHG iterations per instance as of the last solve
+    bool totals_known_ = true;         // host_total_ matches the device
     int32_t* err_ = nullptr;
     SolveParams* sp_ = nullptr;
     double* stage_ = nullptr;
