@@ -403,7 +403,10 @@ def main():
         "config": {"workload": WORKLOAD if args.workload == "zipf-lp" else "general-integer 20k x 50k",
                    "m": m, "n": n, "nnz": nnz, "precision": "mixed (FP32 iterates and SpMV, FP64 "
                    "reductions, restart logic and polish)", "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (~450 MB streamed per iteration)",
+                   "l2": ("inputs larger than L2 (~450 MB streamed per iteration)"
+                          if args.workload == "zipf-lp" else
+                          "L2-resident (~11 MB per iteration): no L2 flush between steps, the "
+                          "roofline is reported but not a bound here"),
                    "tuning": mx["tuning"]},
         "hbm_gbs": round(bytes_iter32 * value / world / 1e9, 1),
         "iterations_per_step": [s["iters"] for s in mx["steps"]],
