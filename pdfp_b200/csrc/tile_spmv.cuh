@@ -309,15 +309,19 @@ __global__ void __launch_bounds__(Op::NT + NRED + 32) tile_spmv_kernel(const Sid
                     MT* v_s = reinterpret_cast<MT*>(buf + cv.lay.off_v) + cv.sh_v;
                     AT* p1 = reinterpret_cast<AT*>(v_s);
                     AT* p2 = reinterpret_cast<AT*>(buf + cv.lay.off_p2);
+                    // one gathered vector: the values are read only after the gathers
+                    // are issued (fewer registers live across their latency); two: the
+                    // values first (the other order spills in the evaluation kernels)
+                    constexpr bool kLate = NV == 1;
                     for (int32_t k = g; k < K; k += UNROLL * NT) {
                         int32_t col[UNROLL];
-                        MT a[UNROLL];
+                        MT a[kLate ? 1 : UNROLL];
                         GT gv[UNROLL][NV > 0 ? NV : 1];
 #pragma unroll
                         for (int q = 0; q < UNROLL; ++q) {
                             const int32_t kk = k + q * NT;
                             col[q] = kk < K ? ci_s[kk] : 0;
-                            a[q] = kk < K ? v_s[kk] : MT(0);
+                            if constexpr (!kLate) a[q] = kk < K ? v_s[kk] : MT(0);
                         }
 #pragma unroll
                         for (int q = 0; q < UNROLL; ++q)
@@ -326,9 +330,10 @@ __global__ void __launch_bounds__(Op::NT + NRED + 32) tile_spmv_kernel(const Sid
                         for (int q = 0; q < UNROLL; ++q) {
                             const int32_t kk = k + q * NT;
                             if (kk < K) {
-                                p1[kk] = mul_rn(static_cast<AT>(a[q]), static_cast<AT>(gv[q][0]));
+                                const MT av = kLate ? v_s[kk] : a[kLate ? 0 : q];
+                                p1[kk] = mul_rn(static_cast<AT>(av), static_cast<AT>(gv[q][0]));
                                 if (NV > 1)
-                                    p2[kk] = mul_rn(static_cast<AT>(a[q]), static_cast<AT>(gv[q][NV > 1 ? NV - 1 : 0]));
+                                    p2[kk] = mul_rn(static_cast<AT>(av), static_cast<AT>(gv[q][NV > 1 ? NV - 1 : 0]));
                             }
                         }
                     }
