@@ -282,6 +282,38 @@ PDFP_API int pdfp_mps_get(const pdfp_mps* p, double* c, double* c0, int32_t* row
                           double* u, int32_t* int_idx);
 PDFP_API int pdfp_mps_destroy(pdfp_mps* p);
 
+/* ---- the pump's constraint-propagation rounding, on the host ----------------
+ * FP 2.0's CPR rounding as the reference runs it on the CPU: activity-based
+ * bound propagation (src/propagation.jl:1-276) behind the guarded two-phase
+ * rounding (src/rounding.jl:117-256), native.  Needs no GPU.
+ * pdfp_rounder_create: the model part (PropagationData, src/propagation.jl:19-84)
+ * from the canonical rows A x <= b (is_le[i] = 1) or A x = b, column indices
+ * strictly ascending within each row, bounds l <= x <= u (infinite allowed),
+ * is_int per column. */
+typedef struct pdfp_rounder pdfp_rounder;
+PDFP_API int pdfp_rounder_create(const pdfp_csr* A, const double* b, const uint8_t* is_le,
+                                 const double* l, const double* u, const uint8_t* is_int,
+                                 pdfp_rounder** out);
+/* One rounding of x_star (n values) into xt (n values) on fresh domains:
+ * xt = x_star; the columns first[0..n_first) are fixed one by one in that order,
+ * each rounded to nearest (ties to even) inside its current domain -- moved by
+ * one toward the domain if that leaves it, or chosen by the row violations when
+ * direction[j] is set (direction may be NULL) -- and propagated after each fix
+ * (_round_sequentially, src/rounding.jl:152-174); with batch_phase set, the
+ * columns batch[0..n_batch) are then all fixed at their rounded values and
+ * propagated once (the guard: *infeasible = 2 and an incomplete xt when that
+ * leaves the domains infeasible); then after[0..n_after) as `first`; finally the
+ * columns int_idx[0..n_int) read their values off the domains (fixed: the bound;
+ * else the rounded clamped x_star).  max_pops caps the rows popped per
+ * propagation (src/propagation.jl:235-244).  Otherwise *infeasible reports the
+ * final domains' state (1: infeasible, 0: not found infeasible). */
+PDFP_API int pdfp_rounder_round(const pdfp_rounder* r, const double* x_star, const int32_t* first,
+                                int32_t n_first, int32_t batch_phase, const int32_t* batch,
+                                int32_t n_batch, const int32_t* after, int32_t n_after,
+                                const int32_t* int_idx, int32_t n_int, const uint8_t* direction,
+                                int64_t max_pops, double* xt, int32_t* infeasible);
+PDFP_API int pdfp_rounder_destroy(pdfp_rounder* r);
+
 /* max_violation(milp, x), src/milp.jl:102-114, on the device: the largest
  * violation of A x <= b (rows with is_eq[i] == 0) and A x = b (is_eq[i] != 0)
  * over the ORIGINAL constraints (caller's numbering, 0-based CSR, ascending

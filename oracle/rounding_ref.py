@@ -1,10 +1,11 @@
-"""Activity-based bound propagation, the engine behind CPR rounding.
+"""Pure-Python restatement of the pump's CPR rounding (src/propagation.jl:1-276,
+src/rounding.jl:117-256).
 
-Host-side (CPU) restatement of src/propagation.jl:1-276.  The pump keeps this
-logic on the CPU; it is written here with plain Python lists (the models it
-runs on per call are small, and the integer/bound arithmetic is kept exactly
-as the reference's: same tolerances, same wake-up cap, FIFO queue, same row
-classes).
+TEST INFRASTRUCTURE ONLY: the checker of the library's native rounder
+(pdfp_rounder_*, rounding.cpp); tests/ and the CPU-baseline legs of bench.py may
+use it, the product package never does.  Plain Python lists and the reference's
+arithmetic in the reference's order: same tolerances, wake-up cap, FIFO queue and
+row classes.  ``round_phases`` takes the same arguments as pdfp_rounder_round.
 """
 from __future__ import annotations
 
@@ -280,3 +281,97 @@ def fix(s: PropagationState, j: int, value: float) -> bool:
 
 def is_fixed(s: PropagationState, j: int) -> bool:
     return abs(s.u[j] - s.l[j]) < BOUND_TOLERANCE
+
+
+# ---- the rounding phases (src/rounding.jl:117-256) --------------------------------
+
+def _round(v: float) -> float:
+    """Julia ``round`` on a Float64: nearest, ties to even (Python's round is ties-to-even)."""
+    return float(round(v))
+
+
+def _clamp(x: float, lo: float, hi: float) -> float:
+    return hi if x > hi else (lo if x < lo else x)
+
+
+def _row_violation(d: PropagationData, i: int, activity: float) -> float:
+    """src/rounding.jl:117-118"""
+    return max(0.0, activity - d.b[i]) if d.is_le[i] else abs(activity - d.b[i])
+
+
+def _guided_value(d: PropagationData, s: PropagationState, j: int, target: float, activity) -> float:
+    """Violation-guided rounding (src/rounding.jl:123-141)."""
+    if not s.u[j] - s.l[j] > BOUND_TOLERANCE:
+        return target
+    lo = float(math.ceil(s.l[j] - BOUND_TOLERANCE))
+    hi = float(math.floor(s.u[j] + BOUND_TOLERANCE))
+    if not hi > lo:
+        return target
+    rows, vals = d.col_rows[j], d.col_vals[j]
+
+    def score(v):
+        t = 0.0
+        for i, a in zip(rows, vals):
+            t += _row_violation(d, i, activity[i] + a * v) - _row_violation(d, i, activity[i])
+        return t
+
+    score_lo = score(lo)
+    score_hi = score(hi)
+    if score_lo < score_hi - 1e-12:
+        return lo
+    if score_hi < score_lo - 1e-12:
+        return hi
+    return target
+
+
+def _add_activity(d: PropagationData, activity, j: int, v: float) -> None:
+    for i, a in zip(d.col_rows[j], d.col_vals[j]):
+        activity[i] += a * v
+
+
+def _round_sequentially(d, s, xt, idx, x_star, direction, activity) -> None:
+    """src/rounding.jl:152-174"""
+    for j in idx:
+        if is_fixed(s, j):
+            xt[j] = s.l[j]
+            continue
+        target = _round(_clamp(x_star[j], s.l[j], s.u[j]))
+        if target < s.l[j] - BOUND_TOLERANCE or target > s.u[j] + BOUND_TOLERANCE:
+            other = _round(_clamp(x_star[j] + (1.0 if target < s.l[j] else -1.0), s.l[j], s.u[j]))
+            target = _clamp(other, s.l[j], s.u[j])
+        if direction is not None and direction[j]:
+            target = _guided_value(d, s, j, target, activity)
+        fix(s, j, target)
+        propagate(s)
+        if direction is not None:
+            _add_activity(d, activity, j, target)
+        xt[j] = target
+
+
+def round_phases(d: PropagationData, x_star, first, batch_phase: bool, batch, after, int_idx,
+                 direction, max_pops: int):
+    """One rounding call, as pdfp_rounder_round: returns (xt, status) with status 2
+    when the batch phase left the domains infeasible, else 1 / 0 for the final
+    domains infeasible / not."""
+    s = PropagationState(d, max_pops)
+    xs = [float(v) for v in x_star]
+    xt = list(xs)
+    activity = None if direction is None else [0.0] * len(d.b)
+    _round_sequentially(d, s, xt, first, xs, direction, activity)
+    if batch_phase:
+        for j in batch:
+            if is_fixed(s, j):
+                xt[j] = s.l[j]
+                continue
+            target = _round(_clamp(xs[j], s.l[j], s.u[j]))
+            fix(s, j, target)
+            if direction is not None:
+                _add_activity(d, activity, j, target)
+            xt[j] = target
+        propagate(s)
+        if s.infeasible:
+            return xt, 2
+    _round_sequentially(d, s, xt, after, xs, direction, activity)
+    for j in int_idx:
+        xt[j] = s.l[j] if is_fixed(s, j) else _round(_clamp(xs[j], s.l[j], s.u[j]))
+    return xt, 1 if s.infeasible else 0

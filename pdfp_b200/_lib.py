@@ -124,6 +124,10 @@ SIGNATURES = {
     "pdfp_mps_dims": (C.c_int, [vp, ip, ip, C.POINTER(C.c_int64), ip]),
     "pdfp_mps_get": (C.c_int, [vp, dp, dp, ip, ip, dp, dp, up, dp, dp, ip]),
     "pdfp_mps_destroy": (C.c_int, [vp]),
+    "pdfp_rounder_create": (C.c_int, [C.POINTER(Csr), dp, up, dp, dp, up, C.POINTER(vp)]),
+    "pdfp_rounder_round": (C.c_int, [vp, dp, ip, C.c_int32, C.c_int32, ip, C.c_int32, ip, C.c_int32,
+                                     ip, C.c_int32, up, C.c_int64, dp, ip]),
+    "pdfp_rounder_destroy": (C.c_int, [vp]),
     "pdfp_checker_create": (C.c_int, [C.POINTER(Csr), dp, up, C.POINTER(vp)]),
     "pdfp_checker_max_violation": (C.c_int, [vp, dp, dp]),
     "pdfp_checker_destroy": (C.c_int, [vp]),

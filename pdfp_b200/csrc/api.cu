@@ -418,3 +418,33 @@ int pdlp_solve_relaxation(const pdfp_csr* A, const double* c, const double* l, c
 }
 
 }  // extern "C"
+
+int pdfp_rounder_create(const pdfp_csr* A, const double* b, const uint8_t* is_le, const double* l,
+                        const double* u, const uint8_t* is_int, pdfp_rounder** out) {
+    return guarded([&] {
+        if (!A || !out || (A->m > 0 && (!b || !is_le || !A->row_ptr)) || (A->n > 0 && (!l || !u || !is_int)))
+            throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        if (A->m < 0 || A->n < 0) throw pdfp::Error(PDFP_E_INVALID, "negative dimension");
+        *out = reinterpret_cast<pdfp_rounder*>(pdfp::rounder_create(A, b, is_le, l, u, is_int));
+    });
+}
+
+int pdfp_rounder_round(const pdfp_rounder* r, const double* x_star, const int32_t* first,
+                       int32_t n_first, int32_t batch_phase, const int32_t* batch, int32_t n_batch,
+                       const int32_t* after, int32_t n_after, const int32_t* int_idx, int32_t n_int,
+                       const uint8_t* direction, int64_t max_pops, double* xt, int32_t* infeasible) {
+    return guarded([&] {
+        if (!r || !x_star || !xt || !infeasible || n_first < 0 || n_batch < 0 || n_after < 0 ||
+            n_int < 0 || (n_first && !first) || (n_batch && !batch) || (n_after && !after) ||
+            (n_int && !int_idx))
+            throw pdfp::Error(PDFP_E_INVALID, "bad argument");
+        pdfp::rounder_round(*reinterpret_cast<const pdfp::Rounder*>(r), x_star, first, n_first,
+                            batch_phase, batch, n_batch, after, n_after, int_idx, n_int, direction,
+                            max_pops, xt, infeasible);
+    });
+}
+
+int pdfp_rounder_destroy(pdfp_rounder* r) {
+    pdfp::rounder_destroy(reinterpret_cast<pdfp::Rounder*>(r));
+    return PDFP_OK;
+}

@@ -31,4 +31,14 @@ Checker* checker_create(const pdfp_csr& A, const double* b, const uint8_t* is_eq
 double checker_max_violation(Checker& c, const double* x);
 void checker_destroy(Checker* c);
 
+// The pump's constraint-propagation rounding on the host (rounding.cpp).
+struct Rounder;
+Rounder* rounder_create(const pdfp_csr* A, const double* b, const uint8_t* is_le, const double* l,
+                        const double* u, const uint8_t* is_int);
+void rounder_destroy(Rounder* r);
+void rounder_round(const Rounder& r, const double* x_star, const int32_t* first, int32_t n_first,
+                   int32_t batch_phase, const int32_t* batch, int32_t n_batch, const int32_t* after,
+                   int32_t n_after, const int32_t* int_idx, int32_t n_int, const uint8_t* direction,
+                   int64_t max_pops, double* xt, int32_t* infeasible);
+
 }  // namespace pdfp

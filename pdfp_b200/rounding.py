@@ -1,21 +1,25 @@
 """Guarded two-phase CPR rounding (CPU), FP 2.0's constraint-propagation rounding.
 
-Host-side restatement of src/rounding.jl:1-256.  The pump keeps rounding on
-the CPU; the integer arithmetic (ties-to-even rounding, stable ranking sort,
-bound tolerances) follows the reference line for line.  Random choices use the
-``numpy.random.Generator`` handed in by the caller, not Julia's MersenneTwister,
-so trajectories that reach the random swaps (iteration >= swap_iteration),
-flips or perturbations differ from the reference's stream.
+Host-side mirror of src/rounding.jl:1-256.  The pump keeps rounding on the CPU;
+the propagation and the fixing phases run natively in libpdfp_b200.so
+(pdfp_rounder_*, rounding.cpp: the reference's tolerances, queue and row classes,
+its arithmetic in its order), while this module keeps the parts that involve the
+caller's random stream and clock: the fractionality ranking with its random swaps
+(stable sort, ties-to-even rounding) and the online batch policy.  Random choices
+use the ``numpy.random.Generator`` handed in by the caller, not Julia's
+MersenneTwister, so trajectories that reach the random swaps (iteration >=
+swap_iteration), flips or perturbations differ from the reference's stream.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 import time
 
 import numpy as np
+import scipy.sparse as sp
 
-from .propagation import (BOUND_TOLERANCE, PropagationData, PropagationState, fix,
-                          is_fixed, propagate)
+from . import _lib as L
 
 
 def _round(v: float) -> float:
@@ -91,10 +95,51 @@ class Rounder:
             self._is_binary[j] = milp.l[j] == 0.0 and milp.u[j] == 1.0
         self._int_idx = milp.int_idx.tolist()
 
-    def _new_state(self) -> PropagationState:
+    def _native(self) -> C.c_void_p:
+        """The library's model part of the propagation (built on first use)."""
         if self.data is None:
-            self.data = PropagationData(self.milp)
-        return PropagationState(self.data, self.max_pops)
+            milp = self.milp
+            A = sp.csr_matrix(milp.A, dtype=np.float64)
+            A.sum_duplicates()
+            A.sort_indices()
+            csr, keep = L.make_csr(A)
+            h = C.c_void_p()
+            is_le = np.ascontiguousarray([s == "le" for s in milp.row_sense], dtype=np.uint8)
+            is_int = np.zeros(len(milp.c), dtype=np.uint8)
+            is_int[milp.int_idx] = 1
+            b, lo, hi = L.f64(milp.b), L.f64(milp.l), L.f64(milp.u)
+            L.check(L.lib().pdfp_rounder_create(C.byref(csr), L.dptr(b), L.uptr(is_le), L.dptr(lo),
+                                                L.dptr(hi), L.uptr(is_int), C.byref(h)))
+            self.data = h
+            self._int_arr = np.ascontiguousarray(self._int_idx, dtype=np.int32)
+        return self.data
+
+    def __del__(self):
+        try:
+            if self.data is not None and self.data.value:
+                L.lib().pdfp_rounder_destroy(self.data)
+                self.data = None
+        except Exception:  # noqa: BLE001 (interpreter shutdown)
+            pass
+
+    def _round_phases(self, x_star, first, batch_phase: bool, batch, after):
+        """One native rounding call (pdfp_rounder_round): (xt, status); status 2: the
+        batch phase left the domains infeasible (xt incomplete), 1: the final
+        domains are infeasible, 0: not found infeasible."""
+        h = self._native()
+        xs = L.f64(x_star)
+        xt = np.empty(len(xs))
+        arr = [np.ascontiguousarray(v, dtype=np.int32) for v in (first, batch, after)]
+        direction = None
+        if self.direction is not None:
+            direction = np.ascontiguousarray(self.direction, dtype=np.uint8)
+        inf = C.c_int32()
+        L.check(L.lib().pdfp_rounder_round(
+            h, L.dptr(xs), L.iptr(arr[0]), len(arr[0]), 1 if batch_phase else 0, L.iptr(arr[1]),
+            len(arr[1]), L.iptr(arr[2]), len(arr[2]), L.iptr(self._int_arr), len(self._int_arr),
+            None if direction is None else L.uptr(direction), min(self.max_pops, 2**63 - 1),
+            L.dptr(xt), C.byref(inf)))
+        return xt, int(inf.value)
 
     def _ranking(self, x_star, rng, iteration: int) -> list:
         """Ascending fractionality, binaries first; random swaps from ``swap_iteration`` on
@@ -111,79 +156,14 @@ class Rounder:
                 ranked[a], ranked[b] = ranked[b], ranked[a]
         return ranked
 
-    def _activity(self):
-        return None if self.direction is None else [0.0] * len(self.milp.b)
-
-
-def _row_violation(d: PropagationData, i: int, activity: float) -> float:
-    """src/rounding.jl:117-118"""
-    return max(0.0, activity - d.b[i]) if d.is_le[i] else abs(activity - d.b[i])
-
-
-def _guided_value(r: Rounder, s: PropagationState, j: int, target: float, activity) -> float:
-    """Violation-guided rounding (src/rounding.jl:123-141)."""
-    if not s.u[j] - s.l[j] > BOUND_TOLERANCE:
-        return target
-    lo = float(math.ceil(s.l[j] - BOUND_TOLERANCE))
-    hi = float(math.floor(s.u[j] + BOUND_TOLERANCE))
-    if not hi > lo:
-        return target
-    d = r.data
-    rows, vals = d.col_rows[j], d.col_vals[j]
-
-    def score(v):
-        t = 0.0
-        for i, a in zip(rows, vals):
-            t += _row_violation(d, i, activity[i] + a * v) - _row_violation(d, i, activity[i])
-        return t
-
-    score_lo = score(lo)
-    score_hi = score(hi)
-    if score_lo < score_hi - 1e-12:
-        return lo
-    if score_hi < score_lo - 1e-12:
-        return hi
-    return target
-
-
-def _add_activity(r: Rounder, activity, j: int, v: float) -> None:
-    for i, a in zip(r.data.col_rows[j], r.data.col_vals[j]):
-        activity[i] += a * v
-
-
-def _round_sequentially(r: Rounder, s: PropagationState, xt, idx, x_star, activity) -> None:
-    """src/rounding.jl:152-174"""
-    for j in idx:
-        if is_fixed(s, j):
-            xt[j] = s.l[j]
-            continue
-        target = _round(_clamp(x_star[j], s.l[j], s.u[j]))
-        if target < s.l[j] - BOUND_TOLERANCE or target > s.u[j] + BOUND_TOLERANCE:
-            other = _round(_clamp(x_star[j] + (1.0 if target < s.l[j] else -1.0), s.l[j], s.u[j]))
-            target = _clamp(other, s.l[j], s.u[j])
-        if activity is not None and r.direction[j]:
-            target = _guided_value(r, s, j, target, activity)
-        fix(s, j, target)
-        propagate(s)
-        if activity is not None:
-            _add_activity(r, activity, j, target)
-        xt[j] = target
-
-
-def _read_integers(r: Rounder, s: PropagationState, xt, x_star):
-    for j in r._int_idx:
-        xt[j] = s.l[j] if is_fixed(s, j) else _round(_clamp(x_star[j], s.l[j], s.u[j]))
-    return xt
 
 
 def round_sequential(r: Rounder, x_star, rng, iteration: int) -> np.ndarray:
     """FP 2.0's CPR of ``x_star`` (src/rounding.jl:191-197)."""
-    s = r._new_state()
     xs = [float(v) for v in x_star]
-    xt = list(xs)
     ranked = r._ranking(xs, rng, iteration)
-    _round_sequentially(r, s, xt, ranked, xs, r._activity())
-    return np.array(_read_integers(r, s, xt, xs))
+    xt, _ = r._round_phases(x_star, ranked, False, [], [])
+    return xt
 
 
 def round_guarded(r: Rounder, x_star, rng, iteration: int) -> np.ndarray:
@@ -195,10 +175,7 @@ def round_guarded(r: Rounder, x_star, rng, iteration: int) -> np.ndarray:
         xt = round_sequential(r, x_star, rng, iteration)
         P.observe_skip((time.perf_counter_ns() - t0) / 1e9)
         return xt
-    s = r._new_state()
     xs = [float(v) for v in x_star]
-    xt = list(xs)
-    activity = r._activity()
     ranked = r._ranking(xs, rng, iteration)
 
     def integral(j):
@@ -218,19 +195,8 @@ def round_guarded(r: Rounder, x_star, rng, iteration: int) -> np.ndarray:
         batch = [j for j in ranked if integral(j)]
         after = [j for j in ranked if not integral(j)]
 
-    _round_sequentially(r, s, xt, before, xs, activity)
-    for j in batch:
-        if is_fixed(s, j):
-            xt[j] = s.l[j]
-            continue
-        target = _round(_clamp(xs[j], s.l[j], s.u[j]))
-        fix(s, j, target)
-        if activity is not None:
-            _add_activity(r, activity, j, target)
-        xt[j] = target
-    propagate(s)
-
-    if s.infeasible:  # the guard: discard the batch
+    xt, status = r._round_phases(x_star, before, True, batch, after)
+    if status == 2:  # the guard: discard the batch
         r.n_fallbacks += 1
         wasted = 0.0 if P is None else (time.perf_counter_ns() - t0) / 1e9
         out = round_sequential(r, x_star, rng, iteration)
@@ -238,8 +204,6 @@ def round_guarded(r: Rounder, x_star, rng, iteration: int) -> np.ndarray:
             P.observe_batch(True, (time.perf_counter_ns() - t0) / 1e9, wasted)
         return out
     r.n_batched += 1
-    _round_sequentially(r, s, xt, after, xs, activity)
-    _read_integers(r, s, xt, xs)
     if P is not None:
         P.observe_batch(False, (time.perf_counter_ns() - t0) / 1e9, 0.0)
-    return np.array(xt)
+    return xt
