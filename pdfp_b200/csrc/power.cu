@@ -1,5 +1,7 @@
 // power.cu -- host driver of the batched power iteration.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "power.cuh"
 
@@ -62,6 +64,36 @@ std::vector<double> power_iteration(const DeviceMatrix& M, DeviceArena& ar,
         ps[p].sigma_sq = 1.0;
     }
     PDFP_CK(cudaMemcpyAsync(b.ps, ps.data(), sizeof(PowerState) * K, cudaMemcpyHostToDevice, stream));
+
+    // small instances: one launch for the whole iteration (power_tiny_kernel)
+    bool tiny = true;
+    int64_t smem_doubles = 1;
+    for (int p = 0; p < K && tiny; ++p) {
+        const int64_t mp = L.row_off[p + 1] - L.row_off[p], np = L.col_off[p + 1] - L.col_off[p];
+        const int64_t nz = L.A.rp[L.row_off[p + 1]] - L.A.rp[L.row_off[p]];
+        if (mp + np > kPowerTinyMaxDim || nz > kPowerTinyMaxNnz) tiny = false;
+        smem_doubles = std::max<int64_t>(smem_doubles, 2 * mp + np);
+    }
+    if (const char* te = std::getenv("PDFP_TINY")) tiny = tiny && te[0] != '0';
+    if (tiny) {
+        const size_t smem = sizeof(double) * static_cast<size_t>(smem_doubles);
+        PDFP_CK(cudaFuncSetAttribute(power_tiny_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+        power_tiny_kernel<<<K, kPowerTinyThreads, smem, stream>>>(b, M.rp_t, M.ci_t, M.v64_t, M.rp_a,
+                                                                   M.ci_a, M.v64_a, M.row_off, M.col_off);
+        PDFP_CK(cudaGetLastError());
+        std::vector<PowerState> hs(K);
+        PDFP_CK(cudaMemcpyAsync(hs.data(), b.ps, sizeof(PowerState) * K, cudaMemcpyDeviceToHost, stream));
+        PDFP_CK(cudaStreamSynchronize(stream));
+        if (iters_out) iters_out->assign(K, 0);
+        for (int p = 0; p < K; ++p) {
+            if (!run[p]) continue;
+            const double s2 = hs[p].sigma_sq;
+            result[p] = std::isnan(s2) ? s2 : std::sqrt(s2 > 0.0 ? s2 : 0.0);
+            if (iters_out) (*iters_out)[p] = hs[p].it;
+        }
+        return result;
+    }
 
     launch_rows(ta.dev, PiInitRows{b}, stream);
     launch_finalize(K, PiInitFin{ta.inst_tile0, b.part, nullptr, nullptr, b}, stream);
