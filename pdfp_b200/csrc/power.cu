@@ -24,6 +24,124 @@ void normal_vector(uint64_t seed, int64_t m, double* out) {
     }
 }
 
+// ---- small instances: the whole power iteration in one launch --------------------
+//
+// When every instance has at most kPowerTinyMaxDim rows + columns and
+// kPowerTinyMaxNnz nonzeros, each iteration's six launches would be latency-bound:
+// instead one block per instance runs every iteration, with eig, nxt and dual in
+// shared memory, the same steps in the same order (PiInitFin, then PiNormalize,
+// PiColOp, PiRowOp, PiDotFin, PiResRows, PiResFin per iteration), rows summed
+// sequentially in storage order and the dot products reduced in a fixed order.
+// The loop ends by the instance's own test or its iteration cap.
+constexpr int kPowerTinyThreads = 256;
+constexpr int64_t kPowerTinyMaxDim = 4096;
+constexpr int64_t kPowerTinyMaxNnz = 65536;
+
+// Sums (a, c) over the block (fixed order); every thread gets the totals.
+__device__ __forceinline__ void power_block_sum2(double& a, double& c, double* red) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a = add_rn(a, __shfl_xor_sync(0xffffffffu, a, o));
+        c = add_rn(c, __shfl_xor_sync(0xffffffffu, c, o));
+    }
+    __syncthreads();  // the previous sum's readers are done with red
+    if ((threadIdx.x & 31) == 0) {
+        red[2 * (threadIdx.x >> 5)] = a;
+        red[2 * (threadIdx.x >> 5) + 1] = c;
+    }
+    __syncthreads();
+    a = 0.0;
+    c = 0.0;
+    for (int w = 0; w < kPowerTinyThreads / 32; ++w) {
+        a = add_rn(a, red[2 * w]);
+        c = add_rn(c, red[2 * w + 1]);
+    }
+}
+
+__global__ void __launch_bounds__(kPowerTinyThreads)
+    power_tiny_kernel(PowerBufs b, const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
+                      const double* __restrict__ v_t, const int32_t* __restrict__ rp_a,
+                      const int32_t* __restrict__ ci_a, const double* __restrict__ v_a,
+                      const int32_t* __restrict__ row_off, const int32_t* __restrict__ col_off) {
+    extern __shared__ double sm[];  // eig[m], nxt[m], dual[n] of this instance
+    __shared__ double red[2 * (kPowerTinyThreads / 32)];
+    __shared__ PowerState st;
+    const int p = blockIdx.x;
+    if (threadIdx.x == 0) st = b.ps[p];
+    __syncthreads();
+    if (st.done) return;  // block-uniform
+    const int32_t r0 = row_off[p], m = row_off[p + 1] - r0;
+    const int32_t c0 = col_off[p], n = col_off[p + 1] - c0;
+    double* eig = sm;
+    double* nxt = sm + m;
+    double* dual = sm + 2 * m;
+    const int t = threadIdx.x;
+
+    // PiInitRows / PiInitFin
+    double a = 0.0, c = 0.0;
+    for (int32_t i = t; i < m; i += kPowerTinyThreads) {
+        const double e = b.eig[r0 + i];
+        eig[i] = e;
+        a += e * e;
+    }
+    power_block_sum2(a, c, red);
+    if (t == 0) {
+        st.nrm = sqrt(a);
+        st.it = 0;
+        st.sigma_sq = 1.0;
+        if (st.max_it <= 0 || st.nrm == 0.0) st.done = 1;
+    }
+    __syncthreads();
+    while (!st.done) {
+        for (int32_t i = t; i < m; i += kPowerTinyThreads) nxt[i] = eig[i] / st.nrm;  // PiNormalize
+        __syncthreads();
+        for (int32_t j = t; j < n; j += kPowerTinyThreads) {  // PiColOp: dual = A' nxt
+            const int32_t row = c0 + j;
+            double sum = 0.0;
+            for (int32_t k = rp_t[row]; k < rp_t[row + 1]; ++k)
+                sum = add_rn(sum, mul_rn(v_t[k], nxt[ci_t[k] - r0]));
+            dual[j] = sum;
+        }
+        __syncthreads();
+        a = 0.0;
+        c = 0.0;
+        for (int32_t i = t; i < m; i += kPowerTinyThreads) {  // PiRowOp: eig = A dual, <nxt, eig>
+            const int32_t row = r0 + i;
+            double sum = 0.0;
+            for (int32_t k = rp_a[row]; k < rp_a[row + 1]; ++k)
+                sum = add_rn(sum, mul_rn(v_a[k], dual[ci_a[k] - c0]));
+            eig[i] = sum;
+            a += nxt[i] * sum;
+        }
+        power_block_sum2(a, c, red);
+        const double sigma_sq = a;  // PiDotFin
+        a = 0.0;
+        c = 0.0;
+        for (int32_t i = t; i < m; i += kPowerTinyThreads) {  // PiResRows
+            const double e = eig[i];
+            const double v = sub_rn(e, mul_rn(sigma_sq, nxt[i]));
+            nxt[i] = v;
+            a += v * v;
+            c += e * e;
+        }
+        power_block_sum2(a, c, red);
+        if (t == 0) {  // PiResFin
+            st.sigma_sq = sigma_sq;
+            st.it += 1;
+            st.res_sq = a;
+            if (sqrt(a) < st.tol) {
+                st.done = 1;
+            } else if (st.it >= st.max_it) {
+                st.done = 1;
+            } else {
+                st.nrm = sqrt(c);
+                if (st.nrm == 0.0) st.done = 1;
+            }
+        }
+        __syncthreads();
+    }
+    if (t == 0) b.ps[p] = st;
+}
+
 std::vector<double> power_iteration(const DeviceMatrix& M, DeviceArena& ar,
                                     const DeviceMatrix::Tiling& ta,
                                     const DeviceMatrix::Tiling& tt, const std::vector<int>& run,
