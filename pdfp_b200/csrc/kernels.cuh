@@ -23,19 +23,19 @@ size_t tile_dyn_smem(const SideDev& s) {
 }
 
 // Persistent grid size for an Op on a side (blocks resident on all SMs).
-template <class Op, bool ASYNC, int NR, int QU = 4>
+template <class Op, bool ASYNC, int NR>
 int tile_grid_of(const SideDev& s, int num_sms) {
     const size_t smem = tile_dyn_smem<Op>(s);
     // The attribute belongs to the kernel, shared by every tiling launched with
     // it: only ever raise it.
     static size_t attr = 0;
     if (smem > attr) {
-        cudaFuncSetAttribute(tile_spmv_kernel<Op, ASYNC, NR, QU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(tile_spmv_kernel<Op, ASYNC, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
         attr = smem;
     }
     int blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_spmv_kernel<Op, ASYNC, NR, QU>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, tile_spmv_kernel<Op, ASYNC, NR>,
                                                   Op::NT + NR + 32, smem);
     const int per_sm = blocks > 0 ? blocks : 1;
     int g = per_sm * num_sms;
@@ -49,18 +49,15 @@ constexpr bool kHalfReducers = HasGatherSrc<Op>::value && sizeof(typename Op::MT
 // async: the Op's gathers by per-thread async copies (gather policy 2); half_red:
 // Op::NT / 2 reducer threads; both ignored for Ops that have no such variant
 template <class Op>
-int tile_grid(const SideDev& s, int num_sms, bool async = false, bool half_red = false,
-              int quads = 4) {
+int tile_grid(const SideDev& s, int num_sms, bool async = false, bool half_red = false) {
     if constexpr (kAsyncEligible<Op>)
         if (async) return tile_grid_of<Op, true, Op::NT>(s, num_sms);
-    if constexpr (kHalfReducers<Op>) {
+    if constexpr (kHalfReducers<Op>)
         if (half_red) return tile_grid_of<Op, false, Op::NT / 2>(s, num_sms);
-        if (quads == 6) return tile_grid_of<Op, false, Op::NT, 6>(s, num_sms);
-    }
     return tile_grid_of<Op, false, Op::NT>(s, num_sms);
 }
 
-template <class Op, bool ASYNC, int NR, int QU = 4>
+template <class Op, bool ASYNC, int NR>
 void launch_tile_k(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap,
                    int carveout) {
     cudaLaunchConfig_t cfg = {};
@@ -82,7 +79,7 @@ void launch_tile_k(const SideDev& s, const Op& op, int grid, cudaStream_t stream
     }
     cfg.attrs = at;
     cfg.numAttrs = na;
-    cudaLaunchKernelEx(&cfg, tile_spmv_kernel<Op, ASYNC, NR, QU>, s, op);  // errors: cudaGetLastError
+    cudaLaunchKernelEx(&cfg, tile_spmv_kernel<Op, ASYNC, NR>, s, op);  // errors: cudaGetLastError
 }
 
 // Share of the SM's unified L1 / shared memory (percent) that `blocks` resident
@@ -98,27 +95,21 @@ int tile_carveout(const SideDev& s, int blocks, int max_smem_per_sm) {
 // overlap: the launch may start while the previous grid on the stream drains
 // (programmatic dependent launch; only directly after another tile-engine launch
 // of a step -- see tile_spmv.cuh).  carveout >= 0: the preferred shared-memory
-// share of the unified L1 (percent) for this launch.  half_red: Op::NT / 2 reducers;
-// quads = 6: 24 gathers in flight per gatherer thread (FP32 steps).
+// share of the unified L1 (percent) for this launch.  half_red: Op::NT / 2 reducers.
 template <class Op>
 void launch_tile(const SideDev& s, const Op& op, int grid, cudaStream_t stream, bool overlap = false,
-                 int carveout = -1, bool half_red = false, int quads = 4) {
+                 int carveout = -1, bool half_red = false) {
     if (s.n_tiles <= 0 || grid <= 0) return;
     if constexpr (kAsyncEligible<Op>)
         if (op.gather_l2 == 2) {
             launch_tile_k<Op, true, Op::NT>(s, op, grid, stream, overlap, carveout);
             return;
         }
-    if constexpr (kHalfReducers<Op>) {
+    if constexpr (kHalfReducers<Op>)
         if (half_red) {
             launch_tile_k<Op, false, Op::NT / 2>(s, op, grid, stream, overlap, carveout);
             return;
         }
-        if (quads == 6) {
-            launch_tile_k<Op, false, Op::NT, 6>(s, op, grid, stream, overlap, carveout);
-            return;
-        }
-    }
     launch_tile_k<Op, false, Op::NT>(s, op, grid, stream, overlap, carveout);
 }
 

@@ -631,9 +631,9 @@ void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
     if (s.engine == 1)
         launch_flat(s.tiling.dev, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red, s.quads);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 256>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
     else
-        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red, s.quads);
+        launch_tile(s.tiling.dev, PrimalOp<T, MAJOR, 128>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
 }
 
 template <typename T, bool MAJOR>
@@ -642,21 +642,21 @@ void Projector::launch_dual(const StepSide& s, int k, bool overlap) {
     if (s.engine == 1)
         launch_flat(s.tiling.dev, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red, s.quads);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 256>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
     else
-        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red, s.quads);
+        launch_tile(s.tiling.dev, DualOp<T, MAJOR, 128>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_, overlap, s.carveout, s.half_red);
 }
 
 // Grid of a step Op family for a tiling (sets the shared-memory attribute of
 // both the MAJOR and the minor kernel).
 template <template <typename, bool, int> class OpT, typename T>
-static int step_grid(const SideDev& d, int nt, int sms, bool async, bool half_red, int quads) {
+static int step_grid(const SideDev& d, int nt, int sms, bool async, bool half_red) {
     if (nt == 256) {
-        tile_grid<OpT<T, false, 256>>(d, sms, async, half_red, quads);
-        return tile_grid<OpT<T, true, 256>>(d, sms, async, half_red, quads);
+        tile_grid<OpT<T, false, 256>>(d, sms, async, half_red);
+        return tile_grid<OpT<T, true, 256>>(d, sms, async, half_red);
     }
-    tile_grid<OpT<T, false, 128>>(d, sms, async, half_red, quads);
-    return tile_grid<OpT<T, true, 128>>(d, sms, async, half_red, quads);
+    tile_grid<OpT<T, false, 128>>(d, sms, async, half_red);
+    return tile_grid<OpT<T, true, 128>>(d, sms, async, half_red);
 }
 
 void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
@@ -683,13 +683,12 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     s.tiling.dev.evict_first = evict_first_ ? 1 : 0;
     const bool async = s.gather_l2 == 2;
     if (!f32 || async) s.half_red = false;  // half-size reducers: FP32 register-gather steps only
-    if (!f32 || async || s.half_red) s.quads = 4;  // 6 quads: the same, full reducers
     if (primal)
-        s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_, async, s.half_red, s.quads)
-                     : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_, async, false, 4);
+        s.grid = f32 ? step_grid<PrimalOp, float>(s.tiling.dev, s.nt, num_sms_, async, s.half_red)
+                     : step_grid<PrimalOp, double>(s.tiling.dev, s.nt, num_sms_, async, false);
     else
-        s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_, async, s.half_red, s.quads)
-                     : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_, async, false, 4);
+        s.grid = f32 ? step_grid<DualOp, float>(s.tiling.dev, s.nt, num_sms_, async, s.half_red)
+                     : step_grid<DualOp, double>(s.tiling.dev, s.nt, num_sms_, async, false);
     // A cap on resident blocks per SM: fewer blocks than shared memory allows, with
     // the unified L1 / shared split asking only for their shared memory, so that
     // the rest stays L1 (the gathers' in-flight misses live there).
@@ -720,7 +719,6 @@ void Projector::autotune(bool f32) {
         int engine, stage, nt, l2, qpt, stages;
         int max_blocks = 0;  // resident blocks per SM (0: as many as fit)
         int half_red = 0;    // 1: nt / 2 reducer threads
-        int quads = 4;       // gathers in flight per gatherer thread / 4
     };
     // tile engine, 4 stages per block: 12-16 KB stages give 3-4 blocks per SM, 24 KB
     // two, 32-48 KB one; 128-thread roles with 2-3 larger stages, 3 blocks per SM;
@@ -743,10 +741,6 @@ void Projector::autotune(bool f32) {
         {0, 12 * 1024, 128, 0, 0, 4, 3}, {0, 28 * 1024, 128, 1, 0, 2, 2}, {0, 24 * 1024, 128, 1, 0, 3, 2},
         {0, 16 * 1024, 128, 0, 0, 3, 3}, {0, 22 * 1024, 128, 1, 0, 2, 3}, {0, 26 * 1024, 128, 1, 0, 2, 3},
         {0, 18 * 1024, 128, 1, 0, 3, 3},
-        // 24 gathers in flight per gatherer thread
-        {0, 22 * 1024, 128, 1, 0, 2, 3, 0, 6}, {0, 24 * 1024, 128, 1, 0, 2, 3, 0, 6},
-        {0, 28 * 1024, 128, 1, 0, 2, 0, 0, 6}, {0, 12 * 1024, 128, 0, 0, 3, 0, 0, 6},
-        {0, 18 * 1024, 128, 0, 0, 3, 3, 0, 6}, {0, 24 * 1024, 128, 0, 0, 2, 3, 0, 6},
         // 256 gatherers with 128 reducers
         {0, 24 * 1024, 256, 0, 0, 2, 0, 1}, {0, 32 * 1024, 256, 1, 0, 2, 0, 1},
         // gather policy 2: per-thread async copies into the stage (FP32 steps)
@@ -771,7 +765,6 @@ void Projector::autotune(bool f32) {
             sides[i].gather_l2 = cands[i].l2;
             sides[i].max_blocks = cands[i].max_blocks;
             sides[i].half_red = cands[i].half_red != 0;
-            sides[i].quads = cands[i].quads;
             prepare_side(sides[i], primal, f32);
             if (sides[i].grid <= 0) empty_side = true;
         }

@@ -71,7 +71,6 @@ class Projector {
         int max_blocks = 0;  // tile engine: resident blocks per SM cap (0: as many as fit)
         int carveout = -1;   // preferred shared-memory share of L1 for that cap (percent)
         bool half_red = false;  // tile engine: nt / 2 reducer threads (FP32 steps)
-        int quads = 4;          // tile engine: 4 * quads gathers in flight per gatherer (4 or 6)
         int stage_bytes = 32 * 1024;
         int nt = 256;
         DeviceMatrix::Tiling tiling;

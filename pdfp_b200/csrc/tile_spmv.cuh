@@ -158,9 +158,7 @@ __device__ __forceinline__ int32_t next_chunk(const SideDev& s, const Op& op, Wo
 // ASYNC (a separate instantiation, so the register-gather path keeps its own register
 // budget): the gatherers fetch by per-thread async copies; eligible Ops only.
 // NRED: reducer threads (a multiple of 32, at most Op::NT); the gatherers are Op::NT.
-// QUADS: quads (4 nonzeros) per gatherer thread and pass on the FP32 path, i.e.
-// 4 * QUADS gathers in flight per thread.
-template <class Op, bool ASYNC = false, int NRED = Op::NT, int QUADS = 4>
+template <class Op, bool ASYNC = false, int NRED = Op::NT>
 __global__ void __launch_bounds__(Op::NT + NRED + 32) tile_spmv_kernel(const SideDev s, const Op op) {
     using MT = typename Op::MT;
     using VT = typename Op::VT;
@@ -241,7 +239,7 @@ __global__ void __launch_bounds__(Op::NT + NRED + 32) tile_spmv_kernel(const Sid
                     const int4* ci4 = reinterpret_cast<const int4*>(buf + cv.lay.off_ci);
                     float4* v4 = reinterpret_cast<float4*>(buf + cv.lay.off_v);
                     const int32_t quads = (sh0 + K + 3) >> 2;
-                    constexpr int QH = QUADS;  // quads per thread per pass
+                    constexpr int QH = 4;  // quads per thread per pass: 16 gathers in flight
                     if constexpr (async) {
                         // async policy: each gathered entry is copied (cp.async, 4 bytes)
                         // over its own column index in the stage, and the products are
