@@ -25,6 +25,7 @@
 #include "controller.cuh"
 #include "power.cuh"
 #include "tiny_steps.cuh"
+#include "medium_steps.cuh"
 #include "projector.hpp"
 
 namespace pdfp {
@@ -35,6 +36,7 @@ constexpr double kFp32TolFloor = 1e-6;  // tighter relative tolerances run in FP
 constexpr int64_t kMixedMinNnz = 1 << 18;  // smaller mixed handles compute in FP64
 constexpr int64_t kTinyMaxDim = 4096;      // rows + columns of a member for the one-launch steps
 constexpr int64_t kTinyMaxNnz = 1 << 16;   // nonzeros of a member for the one-launch steps
+constexpr int64_t kMediumMaxNnz = 1 << 21; // nonzeros of a handle for the cooperative steps
 
 // ---- per-instance state kernels ---------------------------------------------------
 
@@ -424,6 +426,40 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
             const int64_t dim = (L.row_off[p + 1] - L.row_off[p]) + (L.col_off[p + 1] - L.col_off[p]);
             const int64_t nz = L.A.rp[L.row_off[p + 1]] - L.A.rp[L.row_off[p]];
             if (dim > kTinyMaxDim || nz > kTinyMaxNnz) tiny_ = false;
+        }
+    }
+
+    // Medium handles (not tiny, at most kMediumMaxNnz nonzeros; PDFP_MEDIUM=0 / =1
+    // switches this off / on regardless of size): the minor steps of a window run in
+    // one cooperative launch, one block per SM over nonzero-balanced row ranges.
+    {
+        const char* me = std::getenv("PDFP_MEDIUM");
+        medium_ = me ? me[0] == '1' : (!tiny_ && L.NNZ <= kMediumMaxNnz);
+        if (medium_ && tiny_) medium_ = false;
+        if (medium_) {
+            int coop = 0, dev = 0;
+            PDFP_CK(cudaGetDevice(&dev));
+            PDFP_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+            if (!coop) medium_ = false;
+        }
+        if (medium_) {
+            const int G = num_sms_;
+            // each block's share: nonzeros + 4 per row (the epilogue), contiguous rows
+            auto split = [&](const std::vector<int32_t>& rp, int64_t rows) {
+                std::vector<int32_t> part(G + 1, 0);
+                const double total = static_cast<double>(rp[rows]) + 4.0 * static_cast<double>(rows);
+                int64_t r = 0;
+                for (int g = 1; g < G; ++g) {
+                    const double want = total * g / G;
+                    while (r < rows && static_cast<double>(rp[r + 1]) + 4.0 * static_cast<double>(r + 1) <= want) ++r;
+                    part[g] = static_cast<int32_t>(r);
+                }
+                part[G] = static_cast<int32_t>(rows);
+                return part;
+            };
+            part_t_ = ar_.upload(split(L.At.rp, L.N));
+            part_a_ = ar_.upload(split(L.A.rp, L.M));
+            gbar_ = ar_.alloc<unsigned>(4);
         }
     }
 
@@ -1039,6 +1075,31 @@ void Projector::launch_tiny_steps(int i0, int i1) {
     PDFP_CK(cudaGetLastError());
 }
 
+template <typename T>
+void Projector::launch_medium_steps(int i0, int i1) {
+    const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    using POp = PrimalOp<T, false, kMediumThreads>;
+    using DOp = DualOp<T, false, kMediumThreads>;
+    // gathers read L2 (policy 1): the gathered vectors were written by other blocks
+    const POp pop{vecs<T>(), st_, 0, mode, err_, 1};
+    const DOp dop{vecs<T>(), st_, M_.row_off, M_.n_eq, 0, mode, err_, 1};
+    const GridBar bar{gbar_, gbar_ + 1, gbar_ + 2};
+    PDFP_CK(cudaMemsetAsync(gbar_, 0, sizeof(unsigned) * 4, stream_));  // count, generation, abort
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(num_sms_));
+    cfg.blockDim = dim3(kMediumThreads);
+    cfg.stream = stream_;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    PDFP_CK(cudaLaunchKernelEx(&cfg, medium_steps_kernel<POp, DOp>, pop, dop, M_.rp_t, M_.ci_t, M_.rp_a,
+                               M_.ci_a, M_.col_off, M_.row_off, K_, static_cast<const int32_t*>(part_t_),
+                               static_cast<const int32_t*>(part_a_), bar, static_cast<int32_t>(i0),
+                               static_cast<int32_t>(i1)));
+}
+
 void Projector::record_window(int freq, bool with32, bool with64) {
     const int mode32 = MODE_FP32, mode64 = MODE_FP64;
     // a step launch directly after another step launch may overlap its drain
@@ -1077,6 +1138,14 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             // steps 2 .. freq-1 in one launch per precision
             if (with32) launch_tiny_steps<float>(2, freq);
             if (with64) launch_tiny_steps<double>(2, freq);
+            after_step = false;
+            i = freq - 1;
+            continue;
+        }
+        if (medium_ && !sample && i == 2 && freq > 2) {
+            // steps 2 .. freq-1 in one cooperative launch per precision
+            if (with32) launch_medium_steps<float>(2, freq);
+            if (with64) launch_medium_steps<double>(2, freq);
             after_step = false;
             i = freq - 1;
             continue;
@@ -1122,7 +1191,15 @@ cudaGraphExec_t Projector::window_graph(int freq, bool with32, bool with64) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     PDFP_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    record_window(freq, with32, with64);
+    try {
+        record_window(freq, with32, with64);
+    } catch (...) {  // leave the stream out of capture mode before reporting
+        cudaGraph_t partial = nullptr;
+        cudaStreamEndCapture(stream_, &partial);
+        if (partial) cudaGraphDestroy(partial);
+        cudaGetLastError();
+        throw;
+    }
     cudaError_t e = cudaStreamEndCapture(stream_, &graph);
     if (e != cudaSuccess) throw Error(E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     PDFP_CK(cudaGraphInstantiate(&exec, graph, 0));

@@ -103,6 +103,8 @@ class Projector {
     void record_window(int freq, bool with32, bool with64);
     template <typename T>
     void launch_tiny_steps(int i0, int i1);
+    template <typename T>
+    void launch_medium_steps(int i0, int i1);
     cudaGraphExec_t window_graph(int freq, bool with32, bool with64);
 
     int precision_;
@@ -145,6 +147,9 @@ class Projector {
     bool evict_first_ = true;  // step kernels stream the matrix L2 evict-first
     bool overlap_ = false;     // consecutive step launches overlap (programmatic launch)
     bool tiny_ = false;  // every member small: a window's minor steps run in one launch
+    bool medium_ = false;  // a mid-sized handle: the minor steps in one cooperative launch
+    int32_t *part_t_ = nullptr, *part_a_ = nullptr;  // each block's rows of A' and of A
+    unsigned* gbar_ = nullptr;                          // the grid barrier's words
     cudaEvent_t tev_[3] = {nullptr, nullptr, nullptr};     // sampled step kernels (timing mode)
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
 };

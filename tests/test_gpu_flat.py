@@ -236,3 +236,53 @@ def test_half_size_reducer_role_agrees(oracle, monkeypatch):
     monkeypatch.setenv("PDFP_TUNING", "16384,256,0,24576,256,1,3,2,0,0,96,0")
     with pytest.raises(Exception, match="reducers"):
         gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+
+
+@pytest.mark.parametrize("name", ["p0201", "pk1", "gen-ip054"])
+def test_medium_path_fp64_matches_oracle(oracle, examples, name, monkeypatch):
+    """A window's minor steps in one cooperative launch (one block per SM over
+    nonzero-balanced row ranges, grid barriers between the passes), forced on the
+    example models: the FP64 form takes the oracle's steps (same status and
+    iteration count, iterates within 1e-10)."""
+    monkeypatch.setenv("PDFP_TINY", "0")
+    monkeypatch.setenv("PDFP_MEDIUM", "1")
+    m = examples[name]
+    xt = np.round(np.random.default_rng(4).random(len(m.c)) * (np.minimum(m.u, 3) - m.l) + m.l)
+    x, st, cnt, tun, sc, w = project(oracle, m, xt, 1e-6, "fp64", "tile", monkeypatch)
+    xo, so, o = oracle.project(m, xt, tol=1e-6)
+    assert st == so and cnt == o.total_count
+    assert np.abs(x - xo).max() <= 1e-10
+
+
+def test_medium_path_agrees_with_tile_engine_mixed(oracle, monkeypatch):
+    """The cooperative path against the per-step launches on a matrix with rows longer
+    than a block's share of work, in the mixed form, batch of two members: same
+    status, iteration counts within 5%, l1 distances within 1e-3 relative."""
+    milp, _ = synthetic.zipf_lp(seed=3, m=4000, n=20000, nnz=300_000)
+    rng = np.random.default_rng(8)
+    I = milp.int_idx
+    sc, is_eq, is_int, w = oracle.projector_inputs(milp)
+    xts = []
+    for _ in range(2):
+        xt = np.zeros(len(milp.c))
+        xt[I] = np.round(rng.random(len(I)))
+        xts.append(xt)
+    res = {}
+    for med in ("0", "1"):
+        monkeypatch.setenv("PDFP_MEDIUM", med)
+        b = gpu.PDFPBatch([(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w)] * 2,
+                          precision="mixed")
+        for p in range(2):
+            b.set_target(p, xts[p] / sc.D_c)
+        b.solve(SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-4), 1.0)
+        out = []
+        for p in range(2):
+            x = sc.D_c * b.get(p, "pdhg_x")
+            out.append((b.results[p]["status"], b.results[p]["total_count"],
+                        float(np.sum(w[I] * np.abs(x[I] - xts[p][I]) / sc.D_c[I]))))
+        res[med] = out
+        b.close()
+    for p in range(2):
+        assert res["0"][p][0] == res["1"][p][0] == "OPTIMAL"
+        assert abs(res["0"][p][1] - res["1"][p][1]) <= 0.05 * res["0"][p][1] + 64
+        assert res["1"][p][2] == pytest.approx(res["0"][p][2], rel=1e-3)
