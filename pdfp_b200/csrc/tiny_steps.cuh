@@ -41,10 +41,26 @@ __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restric
         AT s = AT(0);
         if (rr < R) {
             const int32_t row = r0 + rr;
-            for (int32_t k = rp[row] + lane; k < rp[row + 1]; k += G) {
-                GT g[1];
-                op.gather(ci[k], g);
-                s = add_rn(s, mul_rn(static_cast<AT>(vals[k]), static_cast<AT>(g[0])));
+            const int32_t end = rp[row + 1];
+            // four of the lane's nonzeros at a time: their index, value and gather
+            // loads are all issued before the first product is added (same order)
+            constexpr int U = 4;
+            for (int32_t k0 = rp[row] + lane; k0 < end; k0 += U * G) {
+                int32_t c[U];
+                AT a[U];
+                GT g[U][1];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int32_t kk = k0 + u * G;
+                    c[u] = kk < end ? ci[kk] : 0;
+                    a[u] = kk < end ? static_cast<AT>(vals[kk]) : AT(0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (k0 + u * G < end) op.gather(c[u], g[u]);
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (k0 + u * G < end) s = add_rn(s, mul_rn(a[u], static_cast<AT>(g[u][0])));
             }
         }
         for (int o = G >> 1; o > 0; o >>= 1) s = add_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
