@@ -2,7 +2,8 @@
 // instances too large for one block and too small to fill the GPU per launch.
 //
 // Between a few thousand and about a million nonzeros a PDHG step launch costs
-// more in launch latency and drain than in work.  Here one block per SM runs
+// more in launch latency and drain than in work.  Here one 1024-thread block per
+// SM runs
 // steps i0 .. i1-1 of an evaluation window: each block owns a fixed, nonzero-
 // balanced range of A' rows (columns) and of A rows, runs the Ops' passes over
 // its ranges (G lanes per row, the Op's own per-row epilogue, as the one-block
@@ -19,7 +20,7 @@
 
 namespace pdfp {
 
-constexpr int kMediumThreads = 256;
+constexpr int kMediumThreads = 1024;  // one block per SM: all of its warps
 constexpr uint64_t kMediumWaitNs = 2000000000ull;  // 2 s
 
 struct GridBar {
@@ -79,7 +80,7 @@ __device__ __forceinline__ void medium_pass(const Op& op, const int32_t* __restr
         if (!op.active(p)) continue;  // block-uniform
         const int32_t a = off[p] > ra ? off[p] : ra;
         const int32_t b = off[p + 1] < rb ? off[p + 1] : rb;
-        if (a < b) tiny_pass(op, rp, ci, a, b, p);
+        if (a < b) tiny_pass<Op, kMediumThreads>(op, rp, ci, a, b, p);
     }
 }
 

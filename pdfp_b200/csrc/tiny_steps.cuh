@@ -17,7 +17,7 @@ namespace pdfp {
 
 constexpr int kTinyThreads = 256;
 
-template <class Op>
+template <class Op, int NTH = kTinyThreads>
 __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restrict__ rp,
                                           const int32_t* __restrict__ ci, int32_t r0, int32_t r1,
                                           int inst) {
@@ -33,8 +33,8 @@ __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restric
     double none[1] = {0.0};
     const int32_t R = r1 - r0;
     int G = 1;
-    while (G < 32 && G * 2 * R <= kTinyThreads) G *= 2;
-    const int groups = kTinyThreads / G;
+    while (G < 32 && G * 2 * R <= NTH) G *= 2;
+    const int groups = NTH / G;
     const int gid = threadIdx.x / G, lane = threadIdx.x & (G - 1);
     for (int32_t b = 0; b < R; b += groups) {
         const int32_t rr = b + gid;
