@@ -2,9 +2,8 @@
 // instances too large for one block and too small to fill the GPU per launch.
 //
 // Between a few thousand and about a million nonzeros a PDHG step launch costs
-// more in launch latency and drain than in work.  Here one 1024-thread block per
-// SM runs
-// steps i0 .. i1-1 of an evaluation window: each block owns a fixed, nonzero-
+// more in launch latency and drain than in work.  Here one 256-thread block per
+// SM runs steps i0 .. i1-1 of an evaluation window: each block owns a fixed, nonzero-
 // balanced range of A' rows (columns) and of A rows, runs the Ops' passes over
 // its ranges (G lanes per row, the Op's own per-row epilogue, as the one-block
 // path does) and meets the other blocks at a grid barrier after each pass.  The
@@ -20,7 +19,7 @@
 
 namespace pdfp {
 
-constexpr int kMediumThreads = 1024;  // one block per SM: all of its warps
+constexpr int kMediumThreads = 256;  // one block per SM (1024 threads measured slower)
 constexpr uint64_t kMediumWaitNs = 2000000000ull;  // 2 s
 
 struct GridBar {
