@@ -1,10 +1,84 @@
 // device.cu -- uploads of the packed matrix and its tilings.
 #include "device.hpp"
 
+#include <cstdlib>
+#include <mutex>
+#include <string>
+
 namespace pdfp {
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+constexpr int kMaxPoolDevices = 64;
+constexpr uint64_t kPoolKeepBytes = 256ull << 20;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+bool g_pool_failed[kMaxPoolDevices] = {};
+int g_pool_enabled = -1;  // -1: not read yet
+
+cudaMemPool_t current_pool() {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_pool_enabled < 0) {
+        const char* e = std::getenv("PDFP_POOL");
+        g_pool_enabled = (e && e[0] == '0') ? 0 : 1;
+    }
+    if (!g_pool_enabled) return nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxPoolDevices) return nullptr;
+    if (g_pools[dev] || g_pool_failed[dev]) return g_pools[dev];
+    int supported = 0;
+    cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev);
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (!supported || cudaMemPoolCreate(&g_pools[dev], &props) != cudaSuccess) {
+        g_pools[dev] = nullptr;
+        g_pool_failed[dev] = true;
+        cudaGetLastError();
+        return nullptr;
+    }
+    uint64_t keep = kPoolKeepBytes;
+    cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    return g_pools[dev];
+}
+}  // namespace
+
+void* arena_malloc(size_t bytes, bool* pooled) {
+    void* p = nullptr;
+    *pooled = false;
+    if (cudaMemPool_t pool = current_pool()) {
+        // on the legacy default stream, then waited for: the memory is zero and
+        // usable from every stream when this returns
+        PDFP_CK(cudaMallocFromPoolAsync(&p, bytes, pool, 0));
+        *pooled = true;
+        cudaError_t e = cudaMemsetAsync(p, 0, bytes, 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(p, 0);
+            throw Error(E_CUDA, std::string("arena zero-fill: ") + cudaGetErrorString(e));
+        }
+        return p;
+    }
+    PDFP_CK(cudaMalloc(&p, bytes));
+    cudaError_t e = cudaMemset(p, 0, bytes);
+    if (e != cudaSuccess) {
+        cudaFree(p);
+        throw Error(E_CUDA, std::string("arena zero-fill: ") + cudaGetErrorString(e));
+    }
+    return p;
+}
+
+void arena_free(const std::vector<void*>& ptrs, const std::vector<bool>& pooled) {
+    // no kernel of any stream may still use the memory (cudaFree's own guarantee)
+    cudaDeviceSynchronize();
+    for (size_t i = 0; i < ptrs.size(); ++i) {
+        if (pooled[i]) cudaFreeAsync(ptrs[i], 0); else cudaFree(ptrs[i]);
+    }
+    cudaStreamSynchronize(0);
+}
 const char* last_error_cstr() { return g_last_error.c_str(); }
 
 __global__ void f64_to_f32_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t n) {

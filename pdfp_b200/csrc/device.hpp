@@ -32,6 +32,16 @@ void set_last_error(const std::string& msg);
         }                                                                                       \
     } while (0)
 
+// Device memory behind the arenas.  By default it comes from a library-owned,
+// stream-ordered memory pool per device that keeps up to 256 MB of freed memory
+// for reuse, so that the many small handles of a pump run (scaling, root LP,
+// projector, power iteration) do not pay a driver allocation and a device-wide
+// free for each of their buffers; PDFP_POOL=0, or a device without memory pools,
+// uses cudaMalloc / cudaFree.  arena_malloc returns zero-filled memory that any
+// stream may use; arena_free waits for the whole device first (as cudaFree does).
+void* arena_malloc(size_t bytes, bool* pooled);
+void arena_free(const std::vector<void*>& ptrs, const std::vector<bool>& pooled);
+
 // Owns device allocations; every buffer is zero-filled and padded by 64 bytes
 // so that 16-byte-rounded bulk copies of any sub-range stay inside it.
 class DeviceArena {
@@ -43,10 +53,10 @@ class DeviceArena {
     template <class T>
     T* alloc(size_t n) {
         size_t bytes = ((n * sizeof(T) + 63) & ~size_t(63)) + 64;
-        void* p = nullptr;
-        PDFP_CK(cudaMalloc(&p, bytes));
+        bool pooled = false;
+        void* p = arena_malloc(bytes, &pooled);
         ptrs_.push_back(p);
-        PDFP_CK(cudaMemset(p, 0, bytes));
+        pooled_.push_back(pooled);
         bytes_ += bytes;
         return static_cast<T*>(p);
     }
@@ -57,14 +67,16 @@ class DeviceArena {
         return d;
     }
     void release() {
-        for (void* p : ptrs_) cudaFree(p);
+        if (!ptrs_.empty()) arena_free(ptrs_, pooled_);
         ptrs_.clear();
+        pooled_.clear();
         bytes_ = 0;
     }
     size_t bytes() const { return bytes_; }
 
   private:
     std::vector<void*> ptrs_;
+    std::vector<bool> pooled_;
     size_t bytes_ = 0;
 };
 
