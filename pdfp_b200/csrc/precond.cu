@@ -12,6 +12,7 @@
 // (two sequential norms, as the reference's loops) run on the device too.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "device.hpp"
@@ -137,6 +138,72 @@ __global__ void rescale_apply_kernel(const double* __restrict__ lb, const double
     }
 }
 
+// Small matrices (at most kScaleTinyMaxDim rows + columns and kScaleTinyMaxNnz
+// nonzeros): every Ruiz round and the Pock-Chambolle pass in one launch of one
+// block -- the same per-row and per-entry operations as the kernels above, in the
+// same order (no value depends on how rows are shared among threads), with block
+// barriers where those kernels end.
+constexpr int64_t kScaleTinyMaxDim = 4096;
+constexpr int64_t kScaleTinyMaxNnz = 65536;
+constexpr int kScaleTinyThreads = 1024;
+
+__global__ void __launch_bounds__(kScaleTinyThreads)
+    scale_tiny_kernel(const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
+                      double* __restrict__ v_a, const int32_t* __restrict__ rp_t,
+                      const int32_t* __restrict__ ci_t, double* __restrict__ v_t, int32_t m,
+                      int32_t n, int32_t ruiz_iterations, double alpha, double* __restrict__ rs,
+                      double* __restrict__ cs, double* __restrict__ D_r, double* __restrict__ D_c) {
+    const int t = threadIdx.x;
+    for (int32_t it = 0; it <= ruiz_iterations; ++it) {
+        const bool pc = it == ruiz_iterations;  // the last pass: Pock-Chambolle
+        for (int32_t i = t; i < m; i += kScaleTinyThreads) {
+            if (pc) {
+                double sum = 0.0;
+                for (int32_t p = rp_a[i]; p < rp_a[i + 1]; ++p) {
+                    const double a = fabs(v_a[p]);
+                    sum = __dadd_rn(sum, alpha == 1.0 ? a : pow(a, alpha));
+                }
+                rs[i] = sum < SCALING_EPSILON ? 1.0 : 1.0 / sqrt(sum);
+            } else {
+                double mx = 0.0;
+                for (int32_t p = rp_a[i]; p < rp_a[i + 1]; ++p) {
+                    const double a = fabs(v_a[p]);
+                    if (a > mx) mx = a;
+                }
+                rs[i] = mx < SCALING_EPSILON ? 1.0 : 1.0 / sqrt(mx);
+            }
+        }
+        for (int32_t j = t; j < n; j += kScaleTinyThreads) {
+            if (pc) {
+                const double e = 2.0 - alpha;
+                double sum = 0.0;
+                for (int32_t p = rp_t[j]; p < rp_t[j + 1]; ++p) {
+                    const double a = fabs(v_t[p]);
+                    sum = __dadd_rn(sum, e == 1.0 ? a : pow(a, e));
+                }
+                cs[j] = sum < SCALING_EPSILON ? 1.0 : 1.0 / sqrt(sum);
+            } else {
+                double mx = 0.0;
+                for (int32_t p = rp_t[j]; p < rp_t[j + 1]; ++p) {
+                    const double a = fabs(v_t[p]);
+                    if (a > mx) mx = a;
+                }
+                cs[j] = mx < SCALING_EPSILON ? 1.0 : 1.0 / sqrt(mx);
+            }
+        }
+        __syncthreads();
+        for (int32_t i = t; i < m; i += kScaleTinyThreads)
+            for (int32_t p = rp_a[i]; p < rp_a[i + 1]; ++p)
+                v_a[p] = __dmul_rn(v_a[p], __dmul_rn(rs[i], cs[ci_a[p]]));
+        for (int32_t j = t; j < n; j += kScaleTinyThreads)
+            for (int32_t p = rp_t[j]; p < rp_t[j + 1]; ++p)
+                v_t[p] = __dmul_rn(v_t[p], __dmul_rn(rs[ci_t[p]], cs[j]));
+        for (int32_t i = t; i < m; i += kScaleTinyThreads) D_r[i] = __dmul_rn(D_r[i], rs[i]);
+        for (int32_t j = t; j < n; j += kScaleTinyThreads) D_c[j] = __dmul_rn(D_c[j], cs[j]);
+        __syncthreads();
+    }
+}
+
 static int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8192))); }
 
 void scale_problem_device(const pdfp_csr& A, const double* c, const double* var_lb,
@@ -167,15 +234,24 @@ void scale_problem_device(const pdfp_csr& A, const double* c, const double* var_
         if (m) mul_inplace_kernel<<<bm, 256>>>(D_r, rs, m);
         if (n) mul_inplace_kernel<<<bn, 256>>>(D_c, cs, n);
     };
-    for (int32_t it = 0; it < ruiz_iterations; ++it) {  // src/preconditioner.jl:36-49
-        if (m) ruiz_scale_kernel<<<bm, 256>>>(M.rp_a, M.v64_a, m, rs);
-        if (n) ruiz_scale_kernel<<<bn, 256>>>(M.rp_t, M.v64_t, n, cs);
+    const char* te = std::getenv("PDFP_TINY");
+    const bool tiny = !(te && te[0] == '0') && static_cast<int64_t>(m) + n <= kScaleTinyMaxDim &&
+                      M.L.NNZ <= kScaleTinyMaxNnz && m > 0 && n > 0;
+    if (tiny) {  // every round in one launch
+        scale_tiny_kernel<<<1, kScaleTinyThreads>>>(M.rp_a, M.ci_a, M.v64_a, M.rp_t, M.ci_t, M.v64_t,
+                                                    m, n, std::max(ruiz_iterations, 0), alpha, rs, cs,
+                                                    D_r, D_c);
+    } else {
+        for (int32_t it = 0; it < ruiz_iterations; ++it) {  // src/preconditioner.jl:36-49
+            if (m) ruiz_scale_kernel<<<bm, 256>>>(M.rp_a, M.v64_a, m, rs);
+            if (n) ruiz_scale_kernel<<<bn, 256>>>(M.rp_t, M.v64_t, n, cs);
+            apply();
+        }
+        // Pock-Chambolle, src/preconditioner.jl:51-64
+        if (m) pc_scale_kernel<<<bm, 256>>>(M.rp_a, M.v64_a, m, alpha, rs);
+        if (n) pc_scale_kernel<<<bn, 256>>>(M.rp_t, M.v64_t, n, 2.0 - alpha, cs);
         apply();
     }
-    // Pock-Chambolle, src/preconditioner.jl:51-64
-    if (m) pc_scale_kernel<<<bm, 256>>>(M.rp_a, M.v64_a, m, alpha, rs);
-    if (n) pc_scale_kernel<<<bn, 256>>>(M.rp_t, M.v64_t, n, 2.0 - alpha, cs);
-    apply();
     PDFP_CK(cudaGetLastError());
     PDFP_CK(cudaDeviceSynchronize());
 
