@@ -539,9 +539,8 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
     PDFP_CK(cudaMemcpy(&st_->stall, &s.stall, sizeof(int32_t), cudaMemcpyHostToDevice));
     graph_ = f32_ ? build_graph<float>(200) : build_graph<double>(200);
 
-    InstFlags* fh = nullptr;
-    PDFP_CK(cudaMallocHost(&fh, sizeof(InstFlags) * 2));
-    try {
+    InstFlags fh[2] = {};  // a few bytes per poll: pageable memory, no page-locked allocation
+    {
         for (;;) {
             PDFP_CK(cudaGraphLaunch(graph_, stream_));
             PDFP_CK(cudaMemcpyAsync(fh, flags_, sizeof(InstFlags), cudaMemcpyDeviceToHost, stream_));
@@ -560,11 +559,7 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
             const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
             if (wall > time_limit + 120.0) throw Error(E_TIMEOUT, "root LP exceeded its time limit by 120 s");
         }
-    } catch (...) {
-        cudaFreeHost(fh);
-        throw;
     }
-    cudaFreeHost(fh);
     PDFP_CK(cudaEventRecord(e1, stream_));
     PDFP_CK(cudaMemcpy(&s, st_, sizeof(s), cudaMemcpyDeviceToHost));
     float ms = 0.f;
