@@ -537,12 +537,22 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
     s.stall = 0;
     PDFP_CK(cudaMemcpy(&st_->best_score, &s.best_score, sizeof(double), cudaMemcpyHostToDevice));
     PDFP_CK(cudaMemcpy(&st_->stall, &s.stall, sizeof(int32_t), cudaMemcpyHostToDevice));
-    graph_ = f32_ ? build_graph<float>(200) : build_graph<double>(200);
+    // a small LP's window is a dozen launches: issue them directly, with no graph to
+    // capture and instantiate per solve; a larger one replays a captured window
+    bool f32_window = f32_;
+    if (!tiny_) graph_ = f32_ ? build_graph<float>(200) : build_graph<double>(200);
+    else if (f32_) prepare_grids<float>();
+    else prepare_grids<double>();
 
     InstFlags fh[2] = {};  // a few bytes per poll: pageable memory, no page-locked allocation
     {
         for (;;) {
-            PDFP_CK(cudaGraphLaunch(graph_, stream_));
+            if (tiny_) {
+                if (f32_window) record<float>(200); else record<double>(200);
+                PDFP_CK(cudaGetLastError());
+            } else {
+                PDFP_CK(cudaGraphLaunch(graph_, stream_));
+            }
             PDFP_CK(cudaMemcpyAsync(fh, flags_, sizeof(InstFlags), cudaMemcpyDeviceToHost, stream_));
             PDFP_CK(cudaMemcpyAsync(&fh[1].status, err_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
             PDFP_CK(cudaStreamSynchronize(stream_));
@@ -552,8 +562,10 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
                 launch_elem(1, static_cast<int64_t>(n_) + m_, LpConvert<float, double>{v32_, v64_, n_, m_}, stream_);
                 lp_set_mode_kernel<<<1, 1, 0, stream_>>>(st_, MODE_FP64);
                 PDFP_CK(cudaGetLastError());
-                cudaGraphExecDestroy(graph_);
-                graph_ = build_graph<double>(200);
+                if (graph_) cudaGraphExecDestroy(graph_);
+                graph_ = nullptr;
+                if (tiny_) prepare_grids<double>(); else graph_ = build_graph<double>(200);
+                f32_window = false;
                 polished_ = true;
             }
             const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
