@@ -1177,17 +1177,37 @@ void Projector::record_window(int freq, bool with32, bool with64) {
     if (with64) launch_elem(K_, maxlen, RestartCopy<double>{v64_, st_, M_.col_off, M_.row_off, mode64}, stream_);
 }
 
-cudaGraphExec_t Projector::window_graph(int freq, bool with32, bool with64) {
-    const int key = freq * 8 + (with32 ? 1 : 0) + (with64 ? 2 : 0) + (timing_ ? 4 : 0);
-    auto it = graphs_.find(key);
-    if (it != graphs_.end()) return it->second;
-    // persistent grid sizes and shared-memory attributes (outside capture)
+// persistent grid sizes and shared-memory attributes of the evaluation kernels
+// (outside any capture)
+void Projector::prepare_window() {
     if (precision_ == PDFP_MIXED) {
         tile_grid<EvalColOp<float, NT_EVAL>>(ev_t_.dev, num_sms_);
         tile_grid<EvalRowOp<float, NT_EVAL>>(ev_a_.dev, num_sms_);
     }
     g_.ec = tile_grid<EvalColOp<double, NT_EVAL>>(ev_t_.dev, num_sms_);
     g_.er = tile_grid<EvalRowOp<double, NT_EVAL>>(ev_a_.dev, num_sms_);
+}
+
+// One evaluation window on the stream: a small handle's window (a dozen launches)
+// is issued directly; any other replays the window's captured graph.
+void Projector::run_window(int freq, bool with32, bool with64) {
+    if (tiny_ && !timing_) {
+        if (!window_ready_) {
+            prepare_window();
+            window_ready_ = true;
+        }
+        record_window(freq, with32, with64);
+        PDFP_CK(cudaGetLastError());
+        return;
+    }
+    PDFP_CK(cudaGraphLaunch(window_graph(freq, with32, with64), stream_));
+}
+
+cudaGraphExec_t Projector::window_graph(int freq, bool with32, bool with64) {
+    const int key = freq * 8 + (with32 ? 1 : 0) + (with64 ? 2 : 0) + (timing_ ? 4 : 0);
+    auto it = graphs_.find(key);
+    if (it != graphs_.end()) return it->second;
+    prepare_window();
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     PDFP_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1295,8 +1315,7 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         bool running = false;
         for (int p = 0; p < K_; ++p) running = running || flags_h_[p].status == ST_RUNNING;
         if (!running) break;
-        cudaGraphExec_t g = window_graph(freq, with32, with64);
-        PDFP_CK(cudaGraphLaunch(g, stream_));
+        run_window(freq, with32, with64);
         PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
         PDFP_CK(cudaMemcpyAsync(&flags_h_[K_].status, err_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
         // the states too, and the end event: the poll that finds every instance

@@ -106,6 +106,9 @@ class Projector {
     template <typename T>
     void launch_medium_steps(int i0, int i1);
     cudaGraphExec_t window_graph(int freq, bool with32, bool with64);
+    void prepare_window();
+    void run_window(int freq, bool with32, bool with64);
+    bool window_ready_ = false;  // prepare_window ran (direct windows)
 
     int precision_;
     int K_ = 0;
