@@ -37,7 +37,6 @@ constexpr int64_t kMixedMinNnz = 1 << 18;  // smaller mixed handles compute in F
 constexpr int64_t kTinyMaxDim = 4096;      // rows + columns of a member for the one-launch steps
 constexpr int64_t kTinyMaxNnz = 1 << 16;   // nonzeros of a member for the one-launch steps
 constexpr int64_t kMediumMaxNnz = 1 << 21; // nonzeros of a handle for the cooperative steps
-constexpr size_t kTinySmemMax = 200 * 1024;  // shared memory for the one-launch steps' iterates
 
 // ---- per-instance state kernels ---------------------------------------------------
 
@@ -427,11 +426,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
             const int64_t dim = (L.row_off[p + 1] - L.row_off[p]) + (L.col_off[p + 1] - L.col_off[p]);
             const int64_t nz = L.A.rp[L.row_off[p + 1]] - L.A.rp[L.row_off[p]];
             if (dim > kTinyMaxDim || nz > kTinyMaxNnz) tiny_ = false;
-            const int64_t vals = 9 * static_cast<int64_t>(L.col_off[p + 1] - L.col_off[p]) +
-                                 3 * static_cast<int64_t>(L.row_off[p + 1] - L.row_off[p]);
-            tiny_smem_values_ = std::max(tiny_smem_values_, vals);
         }
-        if (const char* ts = std::getenv("PDFP_TINY_SMEM")) if (ts[0] == '0') tiny_smem_values_ = 0;
     }
 
     // Medium handles (not tiny, at most kMediumMaxNnz nonzeros; PDFP_MEDIUM=0 / =1
@@ -1072,25 +1067,11 @@ void Projector::ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance
 template <typename T>
 void Projector::launch_tiny_steps(int i0, int i1) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    using POp = PrimalOp<T, false, kTinyThreads>;
-    using DOp = DualOp<T, false, kTinyThreads>;
-    const POp pop{vecs<T>(), st_, 0, mode, err_, 0};
-    const DOp dop{vecs<T>(), st_, M_.row_off, M_.n_eq, 0, mode, err_, 0};
-    // the iterates in shared memory when the largest member's fit
-    const size_t smem = sizeof(T) * static_cast<size_t>(tiny_smem_values_);
-    if (smem > 0 && smem <= kTinySmemMax) {
-        static size_t attr = 0;  // per instantiation: only ever raised
-        if (smem > attr) {
-            PDFP_CK(cudaFuncSetAttribute(tiny_steps_smem_kernel<POp, DOp>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-            attr = smem;
-        }
-        tiny_steps_smem_kernel<POp, DOp><<<K_, kTinyThreads, smem, stream_>>>(
-            pop, dop, M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, i0, i1);
-    } else {
-        tiny_steps_kernel<POp, DOp><<<K_, kTinyThreads, 0, stream_>>>(
-            pop, dop, M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, i0, i1);
-    }
+    tiny_steps_kernel<PrimalOp<T, false, kTinyThreads>, DualOp<T, false, kTinyThreads>>
+        <<<K_, kTinyThreads, 0, stream_>>>(
+        PrimalOp<T, false, kTinyThreads>{vecs<T>(), st_, 0, mode, err_, 0},
+        DualOp<T, false, kTinyThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, 0, mode, err_, 0},
+        M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, i0, i1);
     PDFP_CK(cudaGetLastError());
 }
 

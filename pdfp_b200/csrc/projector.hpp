@@ -150,7 +150,6 @@ class Projector {
     bool evict_first_ = true;  // step kernels stream the matrix L2 evict-first
     bool overlap_ = false;     // consecutive step launches overlap (programmatic launch)
     bool tiny_ = false;  // every member small: a window's minor steps run in one launch
-    int64_t tiny_smem_values_ = 0;  // values of the largest member's iterates (one-launch steps)
     bool medium_ = false;  // a mid-sized handle: the minor steps in one cooperative launch
     int32_t *part_t_ = nullptr, *part_a_ = nullptr;  // each block's rows of A' and of A
     unsigned* gbar_ = nullptr;                          // the grid barrier's words

@@ -94,66 +94,4 @@ __global__ void __launch_bounds__(kTinyThreads)
     }
 }
 
-// The projector's steps with the member's iterates in shared memory for the launch:
-// x, x0, y, y0, l, u, x~, w, x-bar (n each) and z, z0, b (m each) are copied in, the
-// passes run on them (the same operations in the same order), and x, y, x-bar and z
-// are copied back.  Dynamic shared memory: (9 n + 3 m) values of the largest member.
-template <class POp, class DOp>
-__global__ void __launch_bounds__(kTinyThreads)
-    tiny_steps_smem_kernel(POp pop, DOp dop,
-                           const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
-                           const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
-                           const int32_t* __restrict__ col_off, const int32_t* __restrict__ row_off,
-                           int32_t i0, int32_t i1) {
-    using T = typename POp::VT;
-    extern __shared__ __align__(16) unsigned char tiny_smem[];
-    const int p = blockIdx.x;
-    if (!pop.active(p)) return;  // block-uniform
-    const int32_t c0 = col_off[p], c1 = col_off[p + 1], r0 = row_off[p], r1 = row_off[p + 1];
-    const int32_t n = c1 - c0, m = r1 - r0;
-    T* base = reinterpret_cast<T*>(tiny_smem);
-    T* const gn[9] = {pop.v.cx, pop.v.ix, pop.v.cy, pop.v.iy, pop.v.lb, pop.v.ub, pop.v.xt, pop.v.w,
-                      pop.v.rx};
-    T* const gm[3] = {pop.v.cz, pop.v.iz, pop.v.b};
-    T* sn[9];
-    T* sm[3];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) sn[k] = base + k * n;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) sm[k] = base + 9 * n + k * m;
-    for (int32_t j = threadIdx.x; j < n; j += kTinyThreads)
-#pragma unroll
-        for (int k = 0; k < 9; ++k) sn[k][j] = gn[k][c0 + j];
-    for (int32_t i = threadIdx.x; i < m; i += kTinyThreads)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) sm[k][i] = gm[k][r0 + i];
-    __syncthreads();
-    // the Ops address packed indices: point them at the shared copies, shifted
-    POp ps = pop;
-    DOp ds = dop;
-    T** const pn[9] = {&ps.v.cx, &ps.v.ix, &ps.v.cy, &ps.v.iy, &ps.v.lb, &ps.v.ub, &ps.v.xt, &ps.v.w,
-                       &ps.v.rx};
-#pragma unroll
-    for (int k = 0; k < 9; ++k) *pn[k] = sn[k] - c0;
-    ps.v.cz = sm[0] - r0;
-    ds.v.cz = sm[0] - r0;
-    ds.v.iz = sm[1] - r0;
-    ds.v.b = sm[2] - r0;
-    ds.v.rx = sn[8] - c0;
-    for (int32_t i = i0; i < i1; ++i) {
-        ps.k_offset = i;
-        ds.k_offset = i;
-        tiny_pass(ps, rp_t, ci_t, c0, c1, p);  // the A'-side pass (primal update)
-        __syncthreads();
-        tiny_pass(ds, rp_a, ci_a, r0, r1, p);  // the A-side pass (dual update)
-        __syncthreads();
-    }
-    for (int32_t j = threadIdx.x; j < n; j += kTinyThreads) {
-        gn[0][c0 + j] = sn[0][j];  // x
-        gn[2][c0 + j] = sn[2][j];  // y
-        gn[8][c0 + j] = sn[8][j];  // x-bar
-    }
-    for (int32_t i = threadIdx.x; i < m; i += kTinyThreads) gm[0][r0 + i] = sm[0][i];  // z
-}
-
 }  // namespace pdfp
