@@ -58,6 +58,8 @@ def dist_setup():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
+        from pdfp_b200 import gpu
+        gpu.set_device(local)  # the library's own runtime selects the rank's GPU too
     return world, rank, local
 
 

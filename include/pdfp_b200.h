@@ -134,6 +134,10 @@ PDFP_API const char* pdfp_last_error(void);
 /* Name of the CUDA device the library uses (the pump log's "device" line,
  * src/pump.jl:442). */
 PDFP_API int pdfp_device_name(char* buf, int32_t len);
+/* Make `device` the calling thread's CUDA device for this library's later calls
+ * (one process per GPU: each rank selects its own; the library otherwise uses the
+ * thread's current device). */
+PDFP_API int pdfp_set_device(int32_t device);
 /* Version string of this library. */
 PDFP_API const char* pdfp_version(void);
 

@@ -88,6 +88,7 @@ SIGNATURES = {
     "pdfp_default_params": (None, [C.POINTER(Params)]),
     "pdfp_last_error": (C.c_char_p, []),
     "pdfp_device_name": (C.c_int, [C.c_char_p, C.c_int32]),
+    "pdfp_set_device": (C.c_int, [C.c_int32]),
     "pdfp_version": (C.c_char_p, []),
     "pdfp_create": (C.c_int, [C.POINTER(Csr), dp, up, up, dp, dp, dp, dp, C.c_int32,
                               C.POINTER(vp)]),

@@ -92,6 +92,15 @@ const char* pdfp_last_error(void) { return pdfp::last_error_cstr(); }
 
 const char* pdfp_version(void) { return "pdfp_b200 0.1.0 (sm_100a)"; }
 
+int pdfp_set_device(int32_t device) {
+    return guarded([&] {
+        int count = 0;
+        PDFP_CK(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count) throw pdfp::Error(PDFP_E_INVALID, "device index out of range");
+        PDFP_CK(cudaSetDevice(device));
+    });
+}
+
 int pdfp_device_name(char* buf, int32_t len) {
     return guarded([&] {
         require_device();

@@ -70,6 +70,11 @@ def _out(out, size):
     return out
 
 
+def set_device(device: int) -> None:
+    """Select the CUDA device of this thread's later library calls (one per rank)."""
+    L.check(L.lib().pdfp_set_device(int(device)))
+
+
 def _precision_code(precision: str) -> int:
     if precision in ("fp64", "FP64", L.FP64):
         return L.FP64

@@ -10,7 +10,9 @@ trajectories on different ranks agree once per pump iteration on a single flag
 
 This replaces the reference's process-per-trajectory launcher
 (scripts/solve.jl:121-148), which runs independent pump processes and keeps the
-first to finish.
+first to finish.  Each rank should select its GPU before solving
+(``pdfp_b200.gpu.set_device(local_rank)``, as ``torch.cuda.set_device`` does for
+torch).
 """
 from __future__ import annotations
 

@@ -138,3 +138,12 @@ def test_pinned_arrays_round_trip(oracle):
     with pytest.raises(ValueError):
         s.get_unscaled("pdhg_x", out=np.zeros(n - 1))
     del a, out, got  # frees the page-locked blocks
+
+
+def test_set_device_selects_and_validates():
+    from pdfp_b200 import _lib as L
+    gpu.set_device(0)
+    assert gpu.device_name()
+    with pytest.raises(Exception, match="out of range"):
+        gpu.set_device(4096)
+    assert L.lib().pdfp_set_device(-1) != 0
