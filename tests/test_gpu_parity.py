@@ -215,7 +215,13 @@ def test_config1_projection_kkt_and_distance(oracle, precision):
 # ---- batching ------------------------------------------------------------------------
 
 
-def test_batch_equals_single_handles(oracle):
+@pytest.mark.parametrize("path", ["default", "cooperative"])
+def test_batch_equals_single_handles(oracle, monkeypatch, path):
+    """Each member of a batch takes exactly its single-handle steps; "cooperative"
+    forces the one-launch-per-window cooperative path (grid barriers) on both."""
+    if path == "cooperative":
+        monkeypatch.setenv("PDFP_TINY", "0")
+        monkeypatch.setenv("PDFP_MEDIUM", "1")
     milps = [synthetic.covering_p0201_like(s) for s in (1, 2, 3)]
     targets = [np.round(np.random.default_rng(s).random(len(m.c))) for s, m in zip((5, 6, 7), milps)]
     probs, singles = [], []
