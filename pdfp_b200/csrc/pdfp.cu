@@ -429,12 +429,13 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
         }
     }
 
-    // Medium handles (not tiny, at most kMediumMaxNnz nonzeros; PDFP_MEDIUM=0 / =1
-    // switches this off / on regardless of size): the minor steps of a window run in
-    // one cooperative launch, one block per SM over nonzero-balanced row ranges.
+    // PDFP_MEDIUM=1: the minor steps of a window run in one cooperative launch, one
+    // block per SM over nonzero-balanced row ranges.  Off by default: on a 500k-
+    // nonzero handle it measured within run-to-run noise of the per-step launches.
     {
         const char* me = std::getenv("PDFP_MEDIUM");
-        medium_ = me ? me[0] == '1' : (!tiny_ && L.NNZ <= kMediumMaxNnz);
+        medium_ = me && me[0] == '1';
+        (void)kMediumMaxNnz;
         if (medium_ && tiny_) medium_ = false;
         if (medium_) {
             int coop = 0, dev = 0;
