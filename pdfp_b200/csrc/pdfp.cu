@@ -36,7 +36,6 @@ constexpr double kFp32TolFloor = 1e-6;  // tighter relative tolerances run in FP
 constexpr int64_t kMixedMinNnz = 1 << 18;  // smaller mixed handles compute in FP64
 constexpr int64_t kTinyMaxDim = 4096;      // rows + columns of a member for the one-launch steps
 constexpr int64_t kTinyMaxNnz = 1 << 16;   // nonzeros of a member for the one-launch steps
-constexpr int64_t kMediumMaxNnz = 1 << 21; // nonzeros of a handle for the cooperative steps
 
 // ---- per-instance state kernels ---------------------------------------------------
 
@@ -435,7 +434,6 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     {
         const char* me = std::getenv("PDFP_MEDIUM");
         medium_ = me && me[0] == '1';
-        (void)kMediumMaxNnz;
         if (medium_ && tiny_) medium_ = false;
         if (medium_) {
             int coop = 0, dev = 0;
