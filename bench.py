@@ -136,6 +136,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def bench_lib():
+    """libpdfp_bench.so, the benchmark's measurement support (pdfp_measure_gather_rate)."""
+    import ctypes as C
+    L = C.CDLL(os.path.join(ROOT, "pdfp_b200", "lib", "libpdfp_bench.so"))
+    L.pdfp_measure_gather_rate.restype = C.c_int
+    L.pdfp_measure_gather_rate.argtypes = [C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+    L.pdfp_bench_last_error.restype = C.c_char_p
+    return L
+
+
 def measured_hbm_peak():
     try:
         d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -187,10 +197,27 @@ def flip_targets(xt, I, milp, rng, frac=0.05):
     return xt
 
 
-def run_projections(state, xt_seq, x_out, params, timed):
+def host_kkt(prob, state, xt):
+    """compute_residual! (src/pdfp.jl:200-218) re-evaluated in FP64 on the host from the
+    solver's pdhg_x, pdhg_y, pdhg_z and dual_slack: (rel_primal, rel_dual, rel_gap)."""
+    A, At, b, is_eq, is_int, w, D_c = prob
+    xts = xt / D_c
+    x, y, z, ds = (state.get(k) for k in ("pdhg_x", "pdhg_y", "pdhg_z", "dual_slack"))
+    d = A @ x - b
+    viol = np.where(is_eq, np.abs(d), np.maximum(d, 0.0))
+    rel_p = np.linalg.norm(viol) / (1.0 + np.linalg.norm(b))
+    rel_d = np.linalg.norm(At @ z - y - ds) / (1.0 + np.linalg.norm(np.where(is_int, w, 0.0)))
+    l1 = np.sum(np.where(is_int, w * np.abs(x - xts), 0.0))
+    yt = np.sum(np.where(is_int, y * (xts - x), 0.0))
+    gap = abs(yt + z @ d - l1) / (1.0 + np.sum(np.where(is_int, w * np.abs(xts), 0.0)))
+    return float(rel_p), float(rel_d), float(gap)
+
+
+def run_projections(state, xt_seq, x_out, params, timed, kkt_prob=None):
     """Project each target as the pump does -- set_target(x_tilde ./ D_c) -> solve ->
     D_c .* pdhg_x, the scaling on the device -- and collect per-step figures.  The
-    targets and x_out are page-locked host arrays."""
+    targets and x_out are page-locked host arrays.  With kkt_prob, each projection's
+    KKT residuals are re-evaluated in FP64 on the host after its timed interval."""
     out = []
     for xt in xt_seq:
         t0 = time.perf_counter()
@@ -201,11 +228,15 @@ def run_projections(state, xt_seq, x_out, params, timed):
         r = state.last
         out.append({"iters": r["total_count"], "device_ms": r["device_ms"], "wall_s": t1 - t0,
                     "status": r["status"], "polished": r["polished"], "rel_gap": r["rel_gap"],
+                    "fp64_iterations": r["fp64_iterations"], "l1": r["objective_value"],
                     "kernel_ms_primal": r["kernel_ms_primal"], "kernel_ms_dual": r["kernel_ms_dual"],
-                    "kernel_samples": r["kernel_samples"], "x_sum": float(np.sum(x))})
+                    "kernel_samples": r["kernel_samples"], "x_sum": float(np.sum(x)),
+                    "max_singular_value": r["max_singular_value"]})
+        if kkt_prob is not None:
+            out[-1]["host_kkt"] = host_kkt(kkt_prob, state, xt)
         if timed:
             log(f"[bench]   {r['status']} iters={r['total_count']} device={r['device_ms']:.1f}ms "
-                f"wall={1e3 * (t1 - t0):.1f}ms polished={r['polished']}")
+                f"wall={1e3 * (t1 - t0):.1f}ms polished={r['polished']} l1={r['objective_value']:.9g}")
     return out
 
 
@@ -225,20 +256,25 @@ def time_reference_form(sc, w, xt0, is_eq, is_int, warm=20, timed=200):
             "note": "steps only (no evaluation windows), FP64, cuSPARSE SpMV"}
 
 
-def cpu_baseline(sc, w, xt0, is_eq, is_int, threads, iterations, label):
-    """The oracle's PDHG steps on the same scaled problem: iterations/s on `threads` host threads."""
+def cpu_baseline(sc, w, xt0, is_eq, is_int, threads, iterations, label, max_sv):
+    """The oracle's pdfp_solve! (src/pdfp.jl:252-288: steps, evaluation windows, restart
+    tests, PID) on the same scaled problem and first target, cut at `iterations`
+    iterations: iterations/s on `threads` host threads.  The ||A||_2 cache is seeded with
+    the GPU run's estimate (the same algorithm's value), as a pump run has it after its
+    first projection."""
     from oracle import oracle as O
     O.set_threads(threads)
     o = O.OraclePDFP(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w)
+    o.set_max_singular_value(max_sv)
     o.set_target(xt0 / sc.D_c)
-    step = 0.998 / np.sqrt(1.0 + 1.0)  # ||A|| <= 1 after Pock-Chambolle scaling; fixed for timing
-    o.steps(step, 1.0, 1, 2)  # warm the caches
+    p = O.default_params(eps_optimal_relative=1e-4, eps_feasible_relative=1e-5,
+                         iteration_limit=iterations)
     t = time.perf_counter()
-    o.steps(step, 1.0, 3, iterations)
+    o.solve(p, 1.0)
     dt = time.perf_counter() - t
-    return {"value": iterations / dt, "unit": "iters/s", "cores": threads, "kind": "port",
-            "sample": f"{iterations} PDHG iterations of the same projection ({label}), "
-                      f"{dt:.1f}s"}
+    return {"value": o.total_count / dt, "unit": "iters/s", "cores": threads, "kind": "port",
+            "sample": f"the oracle's pdfp_solve! on the first target, {o.total_count} PDHG "
+                      f"iterations with their evaluation and restart tests ({label}), {dt:.1f}s"}
 
 
 def main():
@@ -254,7 +290,10 @@ def main():
     ap.add_argument("--nnz", type=int, default=20_000_000)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-iterations", type=int, default=40)
+    ap.add_argument("--cpu-iterations", type=int, default=200,
+                    help="PDHG iterations of the CPU baseline's sample (one evaluation window)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the batch-uneven and pump-markshare figures of the default line")
     ap.add_argument("--no-refform", action="store_true",
                     help="skip the reference-structured FP64 step (cuSPARSE + 3 kernels)")
     args = ap.parse_args()
@@ -285,6 +324,8 @@ def main():
         pinned.append(a)
     x_out = gpu.pinned_zeros(len(xt0))
     warm, timed = pinned[:args.warmup], pinned[args.warmup:]
+    # the host FP64 re-evaluation of every timed mixed projection (outside its timed interval)
+    kkt_prob = (sc.A, sc.A.T.tocsr(), sc.con_ub, is_eq, is_int, w, sc.D_c)
 
     results = {}
     for precision in (["mixed"] if args.no_fp64 else ["mixed", "fp64"]):
@@ -321,7 +362,8 @@ def main():
         gpu.L.check(gpu.L.lib().pdfp_set_kernel_timing(st._h, 1))
         barrier(world)
         with ClockSampler(local) as clk:
-            steps = run_projections(st, timed, x_out, params, True)
+            steps = run_projections(st, timed, x_out, params, True,
+                                    kkt_prob if precision == "mixed" else None)
         barrier(world)
         iters = sum(s["iters"] for s in steps)
         dev_s = sum(s["device_ms"] for s in steps) / 1e3
@@ -350,6 +392,15 @@ def main():
                                 "iterations_per_step": [s["iters"] for s in ls],
                                 "status_per_step": [s["status"] for s in ls]}
         del st
+
+    # configs 3 and 4 of the metric: batched uneven projections and the small pumps
+    extras = {}
+    if args.workload == "zipf-lp" and not args.no_extra:
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup = min(args.steps, 5), 3
+        extras["batch_uneven"] = batch_uneven(sub, world, rank, local, embed=True)
+        sub.workload = "pump-markshare"
+        extras["pump_markshare"] = pump_bench(sub, world, rank, embed=True)
 
     refform_line = None
     if not args.no_refform:
@@ -397,6 +448,14 @@ def main():
         entries.sort(key=lambda e: -e["mean_launch_ms"])
         roof = dict(entries[0])
         roof["other_kernel"] = entries[1]
+        # the sampled minor steps' two kernels against the whole PDHG iteration (every
+        # step of every window, evaluation and controller included): at most 1
+        ms_iter = 1e3 * mx["dev_s"] / max(mx["tot_iters"] / world, 1)
+        roof["kernels_per_iteration_ms"] = round(mx["kp_ms"] + mx["kd_ms"], 5)
+        roof["iteration_ms"] = round(ms_iter, 5)
+        roof["kernel_share_of_iteration"] = round((mx["kp_ms"] + mx["kd_ms"]) / ms_iter, 4)
+        roof["sampling"] = ("CUDA events around both step kernels of 16 minor steps spread "
+                            "evenly over every evaluation window of the timed solves")
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -425,6 +484,23 @@ def main():
         line["time_speedup_vs_fp64_plain"] = round(fp["dev_s"] / mx["dev_s"], 3)
     if "loose" in results:
         line["mixed_both_tolerances_1e-4"] = results["loose"]
+    # the error of every timed mixed projection: its l1 distance against the plain FP64
+    # form's (pinned to the oracle) on the same target, and its KKT residuals
+    # re-evaluated in FP64 on the host
+    kk = [s["host_kkt"] for s in mx["steps"] if "host_kkt" in s]
+    par = {"tolerance": {"eps_optimal_relative": 1e-4, "eps_feasible_relative": 1e-5},
+           "max_host_kkt": {"rel_primal": max(k[0] for k in kk), "rel_dual": max(k[1] for k in kk),
+                            "rel_gap": max(k[2] for k in kk)} if kk else None,
+           "fp64_iterations_in_mixed": sum(s["fp64_iterations"] for s in mx["steps"]),
+           "polished_steps": sum(s["polished"] for s in mx["steps"])}
+    if "fp64" in results:
+        rels = [abs(a["l1"] - b["l1"]) / abs(b["l1"])
+                for a, b in zip(mx["steps"], results["fp64"]["steps"])]
+        par["max_rel_l1_vs_fp64"] = max(rels)
+        par["mean_rel_l1_vs_fp64"] = float(np.mean(rels))
+        par["reference"] = ("the plain FP64 form on the same targets and tolerance (it takes the "
+                            "oracle's steps: same iteration counts, iterates within 1e-10)")
+    line["parity"] = par
     if refform_line is not None:
         line["fp64_reference_form"] = refform_line
         line["speedup_vs_fp64_reference_form"] = round(value / refform_line["value"], 3)
@@ -432,10 +508,13 @@ def main():
     if mx["kp_ms"] and mx["kd_ms"]:
         # the ceiling that binds a scattered sparsity pattern: random 4-byte gathers, from a
         # vector of the size each kernel gathers from (A'z: z, m entries; A x_bar: x_bar, n)
+        blib = bench_lib()
+
         def gather_peak(entries):
             grate = gpu.C.c_double()
-            gpu.L.check(gpu.L.lib().pdfp_measure_gather_rate((nnz // 4) * 4, entries, 20,
-                                                             gpu.C.byref(grate)))
+            rc = blib.pdfp_measure_gather_rate((nnz // 4) * 4, entries, 20, gpu.C.byref(grate))
+            if rc != 0:
+                raise RuntimeError(f"pdfp_measure_gather_rate: {blib.pdfp_bench_last_error()}")
             return grate.value / 1e9
 
         peaks = {"PrimalOp": gather_peak(m), "DualOp": gather_peak(n)}
@@ -460,10 +539,11 @@ def main():
     windows = mx["iters"] // 200
     line["gpu_launches"] = int(windows * (2 * 200 + 10) + args.steps * 12)
     line["clocks"] = mx["clocks"]
+    line.update(extras)
     if not args.no_cpu_baseline and world == 1:  # the host baseline is measured at N = 1 only
         t = time.time()
         line["cpu_baseline"] = cpu_baseline(sc, w, xt0, is_eq, is_int, 1, args.cpu_iterations,
-                                            "single thread")
+                                            "single thread", mx["steps"][0]["max_singular_value"])
         log(f"[bench] cpu baseline in {time.time() - t:.1f}s")
     else:
         line["cpu_baseline"] = None
@@ -471,7 +551,7 @@ def main():
     barrier(world)
 
 
-def batch_uneven(args, world, rank, local):
+def batch_uneven(args, world, rank, local, embed=False):
     """64 uneven binary covering/packing projections packed into one batch handle.
 
     Instances: n log-uniform in [1000, 200000], m = 0.6 n, 10-40 nonzeros per row
@@ -577,6 +657,8 @@ def batch_uneven(args, world, rank, local):
                               "hbm_gbs_fp32_bytes": round(fp["bytes"] / fp["dev_s"] / world / 1e9, 1)}
         line["speedup_vs_fp64_plain"] = round(value / (fp["iters"] / fp["dev_s"]), 3)
         line["time_speedup_vs_fp64_plain"] = round(fp["dev_s"] / mx["dev_s"], 3)
+    if embed:
+        return line
     print(json.dumps(line), flush=True)
 
 
@@ -592,7 +674,7 @@ PUMP_WORKLOADS = {
 }
 
 
-def pump_bench(args, world, rank):
+def pump_bench(args, world, rank, embed=False):
     """Time to first feasible of the pump on 32 small synthetic models.
 
     pump-markshare: 6 equality knapsack rows over 50 binaries with U{0..99}
@@ -662,36 +744,55 @@ def pump_bench(args, world, rank):
             "cpu_baseline": {"value": round(1e3 * float(np.median(cpu)), 2), "unit": "ms (p50)",
                              "cores": 1, "kind": "port",
                              "sample": "the same batched pump on the CPU oracle, model seeds 1..8"}}
+    if embed:
+        return line
     print(json.dumps(line), flush=True)
 
 
 def reference_arm(args, world, rank):
+    """The reference's CPU path (the oracle's C restatement of pdfp_solve!, every host
+    thread) on the same workload: each step projects the next target of the same
+    sequence as our arm (warm-started from the previous one) with the whole solve
+    loop -- steps, evaluation windows, restart tests, PID -- cut at --cpu-iterations
+    iterations (one evaluation window by default).  The first warm-up step fills the
+    per-run ||A||_2 cache with the oracle's own power iteration (untimed)."""
     if rank != 0:
         return
     milp, sc, w, xt0, I = build_workload(args, scaler="oracle")
     threads = os.cpu_count() or 1
-    per_step = max(1, args.cpu_iterations // 4)
+    per_step = max(1, args.cpu_iterations)
     from oracle import oracle as O
     O.set_threads(threads)
+    rng = np.random.Generator(np.random.PCG64(11))
+    seq = [xt0]
+    for _ in range(args.warmup + args.steps - 1):
+        seq.append(flip_targets(seq[-1], I, milp, rng))
     o = O.OraclePDFP(sc.A, sc.con_ub, milp.is_eq, milp.is_int, sc.var_lb, sc.var_ub, w)
-    o.set_target(xt0 / sc.D_c)
-    step = 0.998 / np.sqrt(2.0)
-    for k in range(args.warmup):
-        o.steps(step, 1.0, 1 + k * per_step, per_step)
+    p = O.default_params(eps_optimal_relative=1e-4, eps_feasible_relative=1e-5,
+                         iteration_limit=per_step)
+    t = time.time()
+    for xt in seq[:args.warmup]:
+        o.set_target(xt / sc.D_c)
+        o.solve(p, 1.0)
+    log(f"[bench] reference warm-up (power iteration included) in {time.time() - t:.1f}s")
+    iters = 0
     t = time.perf_counter()
-    for k in range(args.steps):
-        o.steps(step, 1.0, 1 + (args.warmup + k) * per_step, per_step)
+    for xt in seq[args.warmup:]:
+        o.set_target(xt / sc.D_c)
+        o.solve(p, 1.0)
+        iters += o.total_count
     dt = time.perf_counter() - t
-    value = args.steps * per_step / dt
+    value = iters / dt
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "iters/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * dt / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": "fp64 (the reference's CPU path)"},
             "cpu_baseline": {"value": round(value, 3), "unit": "iters/s", "cores": threads,
-                             "kind": "port", "sample": f"{per_step} PDHG iterations per step of "
-                             "the same projection on the C restatement of the reference's CPU "
-                             f"path, {threads} threads"},
+                             "kind": "port", "sample": f"per step, pdfp_solve! on the next "
+                             f"target cut at {per_step} PDHG iterations (evaluation and restart "
+                             "tests included), on the C restatement of the reference's CPU path, "
+                             f"{threads} threads"},
             "e2e": {"value": round(value, 3), "unit": "iters/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

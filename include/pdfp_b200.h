@@ -53,7 +53,8 @@ extern "C" {
 /* Arithmetic of the iterations.  FP64: plain FP64 form.  MIXED: iterates,
  * matrix values and row accumulation in FP32; KKT/gap/restart reductions,
  * Halpern weights and the reported distance in FP64 on the device; an FP64
- * polish takes over when the FP32 residual stalls above tolerance. */
+ * polish takes over when the FP32 residual stalls above tolerance or reaches
+ * the FP32 floor under a tighter tolerance (pdfp_set_polish). */
 #define PDFP_FP64 0
 #define PDFP_MIXED 1
 
@@ -108,6 +109,7 @@ typedef struct {
     double kernel_ms_primal;     /* timing mode: mean device time of the A'-side step kernel */
     double kernel_ms_dual;       /* timing mode: mean device time of the A-side step kernel */
     int64_t kernel_samples;      /* timing mode: launches sampled per kernel */
+    int64_t fp64_iterations;     /* PDHG iterations of this solve run in FP64 (MIXED: the polish) */
 } pdfp_result;
 
 /* One projection problem (the data of PDFPState, src/pdfp.jl:15-52), already
@@ -206,9 +208,22 @@ PDFP_API int pdfp_shape(const pdfp_handle* h, int32_t instance, int32_t* k, int3
 PDFP_API int pdfp_destroy(pdfp_handle* h);
 
 /* Timing mode: when on, every evaluation window of later solves also records
- * CUDA events around two of its step launches per kernel, and pdfp_result
- * reports their mean durations (benchmark support; off by default). */
+ * CUDA events around both step launches of about sixteen minor steps spread
+ * evenly over the window, and pdfp_result reports the mean duration of each
+ * step kernel over them (benchmark support; off by default). */
 PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
+
+/* Mixed precision (PDFP_MIXED handles): an instance starts each solve in FP32;
+ * the FP64 polish -- the iterates converted to FP64 on the device, the solve
+ * continued in FP64 to its tolerance -- takes over after `stall_evaluations`
+ * evaluations without a 10% improvement of the KKT score (the largest
+ * residual-to-tolerance ratio) while above tolerance, or as soon as the
+ * relative residuals reach `fp32_floor` while the requested tolerance is
+ * tighter.  Defaults 10 and 1e-6.  stall_evaluations = 0 switches the polish
+ * off (an instance whose tolerance is below fp32_floor then runs in FP64 from
+ * the start).  The reference has no mixed form; its loop is pdfp_solve!,
+ * src/pdfp.jl:252-288. */
+PDFP_API int pdfp_set_polish(pdfp_handle* h, int32_t stall_evaluations, double fp32_floor);
 
 /* The step-kernel configuration the autotuner chose at creation.  It times, on
  * the handle's own matrix, the tile engine (shared-memory stage size x threads
@@ -332,15 +347,17 @@ PDFP_API int pdfp_checker_create(const pdfp_csr* A, const double* b, const uint8
 PDFP_API int pdfp_checker_max_violation(pdfp_checker* c, const double* x, double* violation);
 PDFP_API int pdfp_checker_destroy(pdfp_checker* c);
 
-/* Measurement support (no counterpart in the reference): the rate, in gathers
- * per second, at which this GPU serves `nnz` independent random 4-byte loads
- * from an m-entry FP32 vector when indices and values stream in coalesced --
- * the ceiling of a sparse step whose column indices are scattered, measured
- * with the simplest kernel that reaches it (best of `repeats` launches in a
- * few launch shapes).  nnz: a positive multiple of 4 below 2^31.  Allocates
- * and frees its own test data. */
-PDFP_API int pdfp_measure_gather_rate(int64_t nnz, int32_t m, int32_t repeats,
-                                      double* gathers_per_s);
+/* Self-test of the library's bounded device waits (no counterpart in the
+ * reference, whose loop ends only on its time and iteration limits,
+ * src/pdfp.jl:279-282).  Every spin of this library's kernels gives up after a
+ * limit and turns into PDFP_E_TIMEOUT with the CUDA context still usable; no
+ * correct solve reaches those limits.  This call runs the same wait code in a
+ * small kernel whose wait cannot complete -- which = 0: the tile engine's
+ * mbarrier wait, on a phase that gets one arrival fewer than it expects;
+ * which = 1: the cooperative window's grid barrier, expecting one block more
+ * than launched -- with a limit of limit_seconds (0 < limit <= 4), no copy in
+ * flight.  Returns PDFP_E_TIMEOUT when the wait gave up as designed. */
+PDFP_API int pdfp_selftest_bounded_wait(int32_t which, double limit_seconds);
 
 /* estimate_max_singular_value(A, A_t, m; max_iterations, tolerance),
  * src/preconditioner.jl:108-125, on the device. */
@@ -352,15 +369,20 @@ PDFP_API int pdfp_estimate_max_singular_value(const pdfp_csr* A, int32_t max_ite
  * cannot call cudaMalloc: processes whose device memory a framework allocator
  * reserved up front (a new cudaMalloc fails or fragments its pool) and callers
  * that must not trigger the device-wide synchronisation of cudaFree.  A and
- * A' are device CSR arrays (0-based, ascending indices per row); the work
- * vectors live in a fixed 8 MiB array of this library's device memory that
- * every GPU loading the library holds until exit, so 2m + n + 2 must not
- * exceed 1,048,576 (PDFP_E_UNSUPPORTED otherwise).  The first call on a device
- * resolves that array's address and should come before any stream capture.
- * Calls share the array: calls that overlap on the GPU race.  `stream` is a
- * cudaStream_t (NULL: the default stream); the call returns when the result
- * is on the host.  Same algorithm, start vector and summation order as
- * pdfp_estimate_max_singular_value. */
+ * A' are device CSR arrays (0-based, ascending indices per row; none may be
+ * NULL when its side has rows); the work vectors live in a fixed 8 MiB array
+ * of this library's device memory, so 2m + n + 2 must not exceed 1,048,576
+ * (PDFP_E_UNSUPPORTED otherwise).  The driver commits that array on a device
+ * at the first call there (CUDA's default lazy module loading; at library load
+ * under CUDA_MODULE_LOADING=EAGER) and the device keeps it until the process
+ * exits: make one call per device before reserving device memory up front, and
+ * before any stream capture (that call also resolves the array's address for
+ * the calling context).  Calls share the array and it keeps the last call's
+ * contents: calls that overlap on the GPU race.  The iteration runs in one
+ * thread block; near the size limit an iteration costs about a millisecond.
+ * `stream` is a cudaStream_t (NULL: the default stream); the call returns when
+ * the result is on the host.  Same algorithm, start vector and summation order
+ * as pdfp_estimate_max_singular_value. */
 PDFP_API int pdfp_estimate_max_singular_value_noalloc(
     int32_t m, int32_t n, const int32_t* row_ptr, const int32_t* col_idx, const double* val,
     const int32_t* row_ptr_t, const int32_t* col_idx_t, const double* val_t,

@@ -103,6 +103,7 @@ def lib():
         L.or_pdfp_solve.restype = C.c_int32
         L.or_pdfp_get.argtypes = [C.c_void_p, C.c_int32, dp]
         L.or_pdfp_steps.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]
+        L.or_pdfp_set_max_singular_value.argtypes = [C.c_void_p, C.c_double]
         L.or_solve_lp_relaxation.argtypes = [C.c_int32, C.c_int32, ip, ip, dp, dp, dp, dp, dp, up,
                                              C.c_double, C.c_double, C.c_int32, dp, dp,
                                              C.POINTER(OrResult)]
@@ -258,6 +259,10 @@ class OraclePDFP:
 
     def steps(self, step_size, primal_weight, k0, count):
         lib().or_pdfp_steps(self.h, step_size, primal_weight, k0, count)
+
+    def set_max_singular_value(self, sigma):
+        """Seed the per-run ||A||_2 cache (src/pdfp.jl:225-229) with a known estimate."""
+        lib().or_pdfp_set_max_singular_value(self.h, float(sigma))
 
 
 def solve_lp_relaxation(milp, tolerance=1e-2, time_limit=3600.0, cupdlpx_termination=False):

@@ -647,6 +647,8 @@ void or_pdfp_get(const or_pdfp* s, int32_t which, double* out) {
     if (len) memcpy(out, src, sizeof(double) * (size_t)len);
 }
 
+void or_pdfp_set_max_singular_value(or_pdfp* s, double sigma) { s->max_sv = sigma; }
+
 void or_pdfp_steps(or_pdfp* s, double step_size, double primal_weight, int32_t k0, int32_t count) {
     s->step_size = step_size;
     s->r.primal_weight = primal_weight;

@@ -105,6 +105,10 @@ int32_t or_pdfp_solve(or_pdfp* s, const or_params* p, double primal_weight, or_r
 void or_pdfp_get(const or_pdfp* s, int32_t which, double* out);
 /* Run `count` PDHG steps with Halpern offsets k0..k0+count-1 (test hook). */
 void or_pdfp_steps(or_pdfp* s, double step_size, double primal_weight, int32_t k0, int32_t count);
+/* Seed the per-run cache of ||A||_2 that pdfp_solve! fills on its first call
+ * (src/pdfp.jl:225-229), as a pump run that already estimated it has it
+ * (benchmark hook: the CPU baseline times solves, not the estimate). */
+void or_pdfp_set_max_singular_value(or_pdfp* s, double sigma);
 
 /* ---- root LP (src/pdlp.jl) ---- */
 /* solve_lp_relaxation, src/pdlp.jl:381-393, for the canonical MILP rows

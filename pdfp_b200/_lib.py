@@ -70,6 +70,7 @@ class Result(C.Structure):
         ("kernel_ms_primal", C.c_double),
         ("kernel_ms_dual", C.c_double),
         ("kernel_samples", C.c_int64),
+        ("fp64_iterations", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -110,6 +111,8 @@ SIGNATURES = {
     "pdfp_shape": (C.c_int, [vp, C.c_int32, ip, ip, ip]),
     "pdfp_destroy": (C.c_int, [vp]),
     "pdfp_set_kernel_timing": (C.c_int, [vp, C.c_int32]),
+    "pdfp_set_polish": (C.c_int, [vp, C.c_int32, C.c_double]),
+    "pdfp_selftest_bounded_wait": (C.c_int, [C.c_int32, C.c_double]),
     "pdfp_get_tuning": (C.c_int, [vp, ip]),
     "pdfp_get_tuning_table": (C.c_int, [vp, C.POINTER(C.c_float), ip, C.c_int32, ip]),
     "pdfp_get_tuning_stages": (C.c_int, [vp, ip]),
@@ -120,7 +123,6 @@ SIGNATURES = {
     "pdfp_scale_problem": (C.c_int, [C.POINTER(Csr), dp, dp, dp, dp, dp, C.c_int32, C.c_double,
                                      C.c_int32, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]),
     "pdfp_estimate_max_singular_value": (C.c_int, [C.POINTER(Csr), C.c_int32, C.c_double, dp, ip]),
-    "pdfp_measure_gather_rate": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, dp]),
     "pdfp_mps_read": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
     "pdfp_mps_dims": (C.c_int, [vp, ip, ip, C.POINTER(C.c_int64), ip]),
     "pdfp_mps_get": (C.c_int, [vp, dp, dp, ip, ip, dp, dp, up, dp, dp, ip]),

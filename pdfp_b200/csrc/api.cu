@@ -261,6 +261,13 @@ int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on) {
     });
 }
 
+int pdfp_set_polish(pdfp_handle* h, int32_t stall_evaluations, double fp32_floor) {
+    return guarded([&] {
+        if (!h) throw pdfp::Error(PDFP_E_INVALID, "null handle");
+        h->proj->set_polish(stall_evaluations, fp32_floor);
+    });
+}
+
 int pdfp_get_tuning(const pdfp_handle* h, int32_t* out) {
     return guarded([&] {
         if (!h || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");
@@ -390,14 +397,6 @@ int pdfp_checker_max_violation(pdfp_checker* c, const double* x, double* violati
 int pdfp_checker_destroy(pdfp_checker* c) {
     pdfp::checker_destroy(reinterpret_cast<pdfp::Checker*>(c));
     return PDFP_OK;
-}
-
-int pdfp_measure_gather_rate(int64_t nnz, int32_t m, int32_t repeats, double* gathers_per_s) {
-    return guarded([&] {
-        if (!gathers_per_s) throw pdfp::Error(PDFP_E_INVALID, "null output");
-        require_device();
-        *gathers_per_s = pdfp::measure_gather_rate(nnz, m, repeats);
-    });
 }
 
 int pdfp_estimate_max_singular_value(const pdfp_csr* A, int32_t max_iterations, double tolerance,

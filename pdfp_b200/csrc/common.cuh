@@ -159,12 +159,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 
 // Bounded wait on an mbarrier phase.  Returns false (and records the timeout
-// in *err) if the phase did not complete within PDFP_WAIT_LIMIT_NS.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err) {
+// in *err) if the phase did not complete within limit_ns (PDFP_WAIT_LIMIT_NS;
+// the self-test passes a shorter one).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err,
+                                                  uint64_t limit_ns = PDFP_WAIT_LIMIT_NS) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     while (!mbar_try_wait_sleep(bar, parity, 20000u)) {
-        if (globaltimer_ns() - t0 > PDFP_WAIT_LIMIT_NS) {
+        if (globaltimer_ns() - t0 > limit_ns) {
             if (err) atomicExch(err, DEV_ERR_TIMEOUT);
             return false;
         }
@@ -177,11 +179,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // then every thread takes its own acquire with a non-blocking test (already
 // complete, so it passes at once).  Returns false if the wait gave up.
 __device__ __forceinline__ bool group_wait(uint64_t* bar, uint32_t parity, int32_t* err,
-                                           bool elected, int id, int nthreads, int32_t* flag) {
-    if (elected && !mbar_wait_bounded(bar, parity, err)) *flag = 1;
+                                           bool elected, int id, int nthreads, int32_t* flag,
+                                           uint64_t limit_ns = PDFP_WAIT_LIMIT_NS) {
+    if (elected && !mbar_wait_bounded(bar, parity, err, limit_ns)) *flag = 1;
     named_sync(id, nthreads);
     if (*flag) return false;
-    if (!mbar_test_wait(bar, parity)) return mbar_wait_bounded(bar, parity, err);
+    if (!mbar_test_wait(bar, parity)) return mbar_wait_bounded(bar, parity, err, limit_ns);
     return true;
 }
 

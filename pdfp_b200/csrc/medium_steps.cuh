@@ -28,15 +28,18 @@ struct GridBar {
     unsigned* abort;  // raised when a wait gave up
 };
 
-// All blocks of the grid meet; false when the barrier was abandoned.
-__device__ __forceinline__ bool grid_barrier(const GridBar& g, int32_t* err) {
+// All blocks of the grid meet; false when the barrier was abandoned.  `expected`
+// arrivals complete a generation (0: the grid's blocks); the self-test asks for
+// more than it launches, with a short limit, to make the wait run out.
+__device__ __forceinline__ bool grid_barrier(const GridBar& g, int32_t* err, unsigned expected = 0,
+                                             uint64_t limit_ns = kMediumWaitNs) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
         const unsigned my_gen = *reinterpret_cast<volatile unsigned*>(g.gen);
         __threadfence();  // this block's writes before its arrival
-        if (atomicAdd(g.count, 1u) == gridDim.x - 1) {
+        if (atomicAdd(g.count, 1u) == (expected ? expected : gridDim.x) - 1) {
             *g.count = 0;
             __threadfence();
             atomicAdd(g.gen, 1u);
@@ -47,7 +50,7 @@ __device__ __forceinline__ bool grid_barrier(const GridBar& g, int32_t* err) {
                     ok = 0;
                     break;
                 }
-                if (globaltimer_ns() - t0 > kMediumWaitNs) {
+                if (globaltimer_ns() - t0 > limit_ns) {
                     atomicExch(g.abort, 1u);
                     if (err) atomicExch(err, 1);
                     ok = 0;

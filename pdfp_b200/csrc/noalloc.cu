@@ -11,16 +11,32 @@
 // synchronisation of cudaFree would stall them.
 //
 // The scratch array (kNoAllocDoubles FP64 values, 8 MiB) is a file-scope
-// __device__ variable: every GPU that loads the library holds it until the
-// process exits.  Host code cannot use the array's name as a device address;
-// the first call on each device resolves its address with
-// cudaGetSymbolAddress (with that device current) and caches it, so the first
-// call on a device should come before any stream capture.  All calls share
-// the array and it keeps the last call's contents: every call overwrites what
-// it reads before reading it, and calls that overlap on the GPU race on it.
+// __device__ variable.  Under CUDA's lazy module loading (the default) the
+// driver commits it on a device when this file's module is first used there --
+// the first call of the entry point on that device -- or when the library is
+// loaded if CUDA_MODULE_LOADING=EAGER; from then on the device holds it until
+// the process exits.  A caller whose allocator reserves device memory up front
+// should therefore make one call per device before that reservation, and
+// before any stream capture.  Host code cannot use the array's name as a
+// device address: the entry point resolves the address with
+// cudaGetSymbolAddress, with the caller's device current, once per CUDA
+// context (keyed by the context's unique id, so a context created after
+// cudaDeviceReset, or a non-primary context, resolves its own address).  All
+// calls share the array and it keeps the last call's contents: every call
+// overwrites what it reads before reading it, and calls that overlap on the
+// GPU race on it.
+//
+// Cost: the whole iteration runs in one 1024-thread block (one SM), reading A
+// and A' once per iteration; at the scratch limit (2m + n + 2 = 2^20 values,
+// e.g. 349k rows x 349k columns) with a few million nonzeros an iteration
+// takes on the order of a millisecond, so the 5000-iteration cap of the
+// reference's default costs seconds there.  It is meant for small and
+// mid-sized matrices.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -31,29 +47,58 @@
 namespace pdfp {
 
 constexpr int64_t kNoAllocDoubles = int64_t(1) << 20;  // 8 MiB per device: 2m + n + 2 values
-constexpr int kNoAllocMaxDevices = 64;
 constexpr int kNoAllocThreads = 1024;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-static std::mutex g_noalloc_mu;
-static double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+// The driver's current-context query, reached through the runtime so that the
+// library links no driver library of its own.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
-// Device address of the scratch array on the current device (resolved once
-// per device, with that device current).
-static double* noalloc_scratch_address() {
-    int dev = 0;
-    PDFP_CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoAllocMaxDevices) throw Error(E_UNSUPPORTED, "device ordinal too large");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            throw Error(E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-        g_noalloc_addr[dev] = static_cast<double*>(p);
+static std::mutex g_noalloc_mu;
+static std::map<unsigned long long, double*> g_noalloc_addr;  // context id -> scratch address
+
+// Unique id of the calling thread's current CUDA context (0 when none is current).
+static unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) !=
+                cudaSuccess || q1 != cudaDriverEntryPointSuccess || !f1 ||
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) !=
+                cudaSuccess || q2 != cudaDriverEntryPointSuccess || !f2)
+            throw Error(E_CUDA, "the driver's context queries are unavailable");
+        get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        get_id = reinterpret_cast<CtxGetIdFn>(f2);
     }
-    return g_noalloc_addr[dev];
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    unsigned long long id = 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) throw Error(E_CUDA, "cuCtxGetId failed");
+    return id;
+}
+
+// Device address of the scratch array in the current context: resolved with
+// cudaGetSymbolAddress (with the caller's device current) the first time a
+// context calls, then taken from the cache.
+static double* noalloc_scratch_address() {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    unsigned long long id = current_context_id();
+    if (id != 0) {
+        auto it = g_noalloc_addr.find(id);
+        if (it != g_noalloc_addr.end()) return it->second;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // binds a context if none is current
+    if (e != cudaSuccess || !p)
+        throw Error(E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    id = current_context_id();
+    if (id != 0) g_noalloc_addr[id] = static_cast<double*>(p);
+    return static_cast<double*>(p);
 }
 
 __device__ __forceinline__ uint64_t splitmix64_at(uint64_t seed, uint64_t k) {
@@ -153,8 +198,9 @@ extern "C" int pdfp_estimate_max_singular_value_noalloc(
                                   " FP64 scratch values; its fixed scratch holds " +
                                   std::to_string(pdfp::kNoAllocDoubles) + " (8 MiB)");
         if (!sigma) throw pdfp::Error(PDFP_E_INVALID, "null output");
-        if ((m > 0 && !row_ptr) || (n > 0 && !row_ptr_t))
-            throw pdfp::Error(PDFP_E_INVALID, "null row pointers");
+        // the nonzero count lives on the device: any row (column) may hold some
+        if ((m > 0 && (!row_ptr || !col_idx || !val)) || (n > 0 && (!row_ptr_t || !col_idx_t || !val_t)))
+            throw pdfp::Error(PDFP_E_INVALID, "null matrix array (row pointers, column indices or values)");
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
             throw pdfp::Error(PDFP_E_NODEVICE, "no CUDA device available");

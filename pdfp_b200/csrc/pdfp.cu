@@ -31,8 +31,6 @@
 namespace pdfp {
 
 constexpr int NT_EVAL = 256;
-constexpr int STALL_EVALS = 10;  // evaluations without 10% KKT progress before the FP64 polish
-constexpr double kFp32TolFloor = 1e-6;  // tighter relative tolerances run in FP64 from the start
 constexpr int64_t kMixedMinNnz = 1 << 18;  // smaller mixed handles compute in FP64
 constexpr int64_t kTinyMaxDim = 4096;      // rows + columns of a member for the one-launch steps
 constexpr int64_t kTinyMaxNnz = 1 << 16;   // nonzeros of a member for the one-launch steps
@@ -79,7 +77,9 @@ __global__ void solve_init_kernel(InstState* st, InstFlags* fl, const SolveParam
     s.mode = q.mode;
     s.best_score = INFINITY;
     s.stall = 0;
-    s.polish_windows = 0;
+    s.stall_limit = q.stall_limit;
+    s.fp32_floor = q.fp32_floor;
+    s.fp64_iters = 0;
     s.do_restart = 0;
     s.restart_now = 0;
     s.restarts = 0;
@@ -169,6 +169,7 @@ struct Controller {
         s.rel_gap = fabs(a[5] + a[9] - a[4]) / s.gap_den;
         s.inner += s.freq;
         s.total += s.freq;
+        if (s.mode == MODE_FP64) s.fp64_iters += s.freq;
         s.restart_now = 0;
         int32_t request = 0;
         if (s.rel_p <= s.eps_feas && s.rel_d <= s.eps_opt && s.rel_gap <= s.eps_opt) {
@@ -187,17 +188,22 @@ struct Controller {
             s.tau = s.step_size / s.primal_weight;
             s.sigma = s.step_size * s.primal_weight;
             if (s.total >= s.iter_limit) s.status = ST_ITERATION_LIMIT;
-            if (s.status == ST_RUNNING && s.mode == MODE_FP32 && polish) {
-                // FP32 progress test: switch this instance to the FP64 form when
-                // its KKT score has not improved by 10% over STALL_EVALS evaluations.
+            if (s.status == ST_RUNNING && s.mode == MODE_FP32 && polish && s.stall_limit > 0) {
+                // End of the FP32 phase: the FP64 polish takes over from the FP32
+                // iterate when the KKT score (largest residual / tolerance ratio) has
+                // not improved by 10% over stall_limit evaluations, or when the
+                // residuals have reached the FP32 floor while the tolerance asks for
+                // more than FP32 iterates carry.
                 const double score = fmax(s.rel_p / s.eps_feas, fmax(s.rel_d / s.eps_opt, s.rel_gap / s.eps_opt));
+                const double ff = fmax(s.eps_feas, s.fp32_floor), fo = fmax(s.eps_opt, s.fp32_floor);
+                const double score32 = fmax(s.rel_p / ff, fmax(s.rel_d / fo, s.rel_gap / fo));
                 if (score < 0.9 * s.best_score) {
                     s.best_score = score;
                     s.stall = 0;
                 } else {
                     s.stall += 1;
                 }
-                if (s.stall >= STALL_EVALS && score > 1.0) request = 1;
+                if (score > 1.0 && (s.stall >= s.stall_limit || score32 <= 1.0)) request = 1;
             }
         }
         fl[p] = InstFlags{s.status, s.mode, request, 0};
@@ -915,6 +921,14 @@ Projector::~Projector() {
     if (stream_) cudaStreamDestroy(stream_);
 }
 
+void Projector::set_polish(int32_t stall_evaluations, double fp32_floor) {
+    if (stall_evaluations < 0) throw Error(E_INVALID, "stall_evaluations must be >= 0");
+    if (!(fp32_floor > 0.0) || !(fp32_floor < 1.0))
+        throw Error(E_INVALID, "fp32_floor must lie in (0, 1)");
+    stall_limit_ = stall_evaluations;
+    fp32_floor_ = fp32_floor;
+}
+
 void Projector::check_instance(int p) const {
     if (p < 0 || p >= K_) throw Error(E_INVALID, "instance index out of range");
 }
@@ -1099,6 +1113,15 @@ void Projector::launch_medium_steps(int i0, int i1) {
                                static_cast<int32_t>(i1)));
 }
 
+// Timing mode samples the minor steps 2, 2 + every, 2 + 2 every, ... (at most
+// kTimedSteps of them) of a window of `freq` steps.
+int Projector::timed_step_every(int freq) { return std::max(1, (freq - 2) / kTimedSteps); }
+int Projector::timed_step_count(int freq) {
+    if (freq < 3) return 0;
+    const int every = timed_step_every(freq);
+    return std::min(kTimedSteps, (freq - 2 + every - 1) / every);
+}
+
 void Projector::record_window(int freq, bool with32, bool with64) {
     const int mode32 = MODE_FP32, mode64 = MODE_FP64;
     // a step launch directly after another step launch may overlap its drain
@@ -1130,7 +1153,12 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             launch_tile(ev_a_.dev, EvalRowOp<double, NT_EVAL>{v64_, ed_, st_, M_.row_off, M_.n_eq, which, mode64, err_}, g_.er, stream_);
         }
     };
+    // timing mode: events around both kernels of the sampled minor steps (about
+    // sixteen, spread evenly over steps 2 .. freq-1, so that the mean is the
+    // window's average step rather than the one after a restart)
     const bool sample = timing_ && freq >= 3 && (with32 != with64);
+    const int sample_every = timed_step_every(freq);
+    int n_sampled = 0;
     for (int i = 1; i <= freq; ++i) {
         const bool major = (i == 1 || i == freq);
         if (tiny_ && !sample && i == 2 && freq > 2) {
@@ -1149,16 +1177,17 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             i = freq - 1;
             continue;
         }
-        if (sample && i == 2) {
-            // events around one minor step of each kernel (timing mode)
+        if (sample && !major && (i - 2) % sample_every == 0 && n_sampled < kTimedSteps) {
+            cudaEvent_t* e = &tev_[3 * n_sampled];
             after_step = false;
-            PDFP_CK(cudaEventRecordWithFlags(tev_[0], stream_, cudaEventRecordExternal));
+            PDFP_CK(cudaEventRecordWithFlags(e[0], stream_, cudaEventRecordExternal));
             if (with32) prim32(i, major); else prim64(i, major);
             after_step = false;
-            PDFP_CK(cudaEventRecordWithFlags(tev_[1], stream_, cudaEventRecordExternal));
+            PDFP_CK(cudaEventRecordWithFlags(e[1], stream_, cudaEventRecordExternal));
             if (with32) dual32(i, major); else dual64(i, major);
             after_step = false;
-            PDFP_CK(cudaEventRecordWithFlags(tev_[2], stream_, cudaEventRecordExternal));
+            PDFP_CK(cudaEventRecordWithFlags(e[2], stream_, cudaEventRecordExternal));
+            ++n_sampled;
             continue;
         }
         if (with32) { prim32(i, major); dual32(i, major); }
@@ -1259,11 +1288,14 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         s.primal_weight = primal_weights[p];
         s.iter_limit = q.iteration_limit;
         s.freq = q.termination_evaluation_frequency;
-        // FP32 iterates carry about seven significant digits: a mixed handle runs an
-        // instance whose tolerance asks for more (below kFp32TolFloor) in FP64 from
-        // the start instead of reaching the FP64 polish through a stall.
-        const bool tight = std::min(q.eps_optimal_relative, q.eps_feasible_relative) < kFp32TolFloor;
-        s.mode = precision_ == PDFP_MIXED && !tight ? MODE_FP32 : MODE_FP64;
+        // A mixed handle starts every instance in FP32.  FP32 iterates carry about
+        // seven significant digits: an instance whose tolerance asks for more than
+        // the FP32 floor gets there through the FP64 polish (see the controller);
+        // with the polish switched off it runs in FP64 from the start instead.
+        const bool tight = std::min(q.eps_optimal_relative, q.eps_feasible_relative) < fp32_floor_;
+        s.mode = precision_ == PDFP_MIXED && (stall_limit_ > 0 || !tight) ? MODE_FP32 : MODE_FP64;
+        s.stall_limit = stall_limit_;
+        s.fp32_floor = fp32_floor_;
         sv_it = q.sv_max_iterations;
         sv_tol = q.sv_tolerance;
         max_time = std::max(max_time, q.time_limit);
@@ -1310,6 +1342,7 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     int32_t dev_err = 0;
     double kp_sum = 0.0, kd_sum = 0.0;
     int64_t k_samples = 0;
+    const int n_timed = timed_step_count(freq);
     for (;;) {
         bool running = false;
         for (int p = 0; p < K_; ++p) running = running || flags_h_[p].status == ST_RUNNING;
@@ -1326,12 +1359,14 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         dev_err = flags_h_[K_].status;
         if (dev_err) throw Error(E_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
         if (timing_ && freq >= 3 && (with32 != with64)) {
-            float a = 0.f, b = 0.f;
-            PDFP_CK(cudaEventElapsedTime(&a, tev_[0], tev_[1]));
-            PDFP_CK(cudaEventElapsedTime(&b, tev_[1], tev_[2]));
-            kp_sum += a;
-            kd_sum += b;
-            ++k_samples;
+            for (int t = 0; t < n_timed; ++t) {
+                float a = 0.f, b = 0.f;
+                PDFP_CK(cudaEventElapsedTime(&a, tev_[3 * t], tev_[3 * t + 1]));
+                PDFP_CK(cudaEventElapsedTime(&b, tev_[3 * t + 1], tev_[3 * t + 2]));
+                kp_sum += a;
+                kd_sum += b;
+                ++k_samples;
+            }
         }
         // FP64 polish for instances whose FP32 progress stalled
         for (int p = 0; p < K_; ++p) {
@@ -1374,6 +1409,7 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         r.fixed_point_error = s.fpe;
         r.objective_value = s.l1;
         r.polished = polished_.count(p) ? 1 : 0;
+        r.fp64_iterations = s.fp64_iters;
         r.precision = s.mode == MODE_FP32 ? PDFP_MIXED : PDFP_FP64;
         r.device_ms = solve_ms;
         r.kernel_ms_primal = k_samples ? kp_sum / k_samples : 0.0;

@@ -49,7 +49,11 @@ class Projector {
     void get_vector(int p, int which, double* out, bool unscaled = false);
     void profile_step(int iterations, float* ms_primal, float* ms_dual, double* bytes_primal,
                       double* bytes_dual);
-    void set_polish(bool on) { polish_enabled_ = on ? 1 : 0; }
+    // Mixed precision: the FP32 phase of an instance ends, and the FP64 polish takes
+    // over, after stall_evaluations evaluations without a 10% KKT improvement while
+    // above tolerance (0: never), or once its residuals reach fp32_floor (relative)
+    // while the requested tolerance is tighter.
+    void set_polish(int32_t stall_evaluations, double fp32_floor);
     // Chosen step-kernel configurations: {stage_bytes, threads, tiles} for the
     // A'-side and the A-side kernel of the handle's base precision.
     void tuning(int32_t* out) const;
@@ -101,6 +105,8 @@ class Projector {
     void load_cols(int p, T* dst, T* dst2, bool unscaled);
     void ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance);
     void record_window(int freq, bool with32, bool with64);
+    static int timed_step_every(int freq);
+    static int timed_step_count(int freq);
     template <typename T>
     void launch_tiny_steps(int i0, int i1);
     template <typename T>
@@ -141,6 +147,8 @@ class Projector {
     std::vector<bool> has_unscale_;
     std::set<int> polished_;
     int32_t polish_enabled_ = 1;
+    int32_t stall_limit_ = 10;   // evaluations without 10% KKT progress before the FP64 polish
+    double fp32_floor_ = 1e-6;  // relative residual the FP32 phase aims for under a tighter tolerance
     struct Grids {
         int ec = 0, er = 0;
     } g_;
@@ -153,7 +161,8 @@ class Projector {
     bool medium_ = false;  // a mid-sized handle: the minor steps in one cooperative launch
     int32_t *part_t_ = nullptr, *part_a_ = nullptr;  // each block's rows of A' and of A
     unsigned* gbar_ = nullptr;                          // the grid barrier's words
-    cudaEvent_t tev_[3] = {nullptr, nullptr, nullptr};     // sampled step kernels (timing mode)
+    static constexpr int kTimedSteps = 16;                 // minor steps sampled per window (timing mode)
+    cudaEvent_t tev_[3 * kTimedSteps] = {};                // around each sampled step's two kernels
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
 };
 

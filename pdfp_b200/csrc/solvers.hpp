@@ -22,8 +22,6 @@ void solve_lp_relaxation_device(const pdfp_csr& A, const double* c, const double
                                 double tolerance, double time_limit, bool cupdlpx, int precision,
                                 double* x_out, double* dual_slack_out, pdfp_result* r);
 
-// Random-gather ceiling of the current GPU (gatherprobe.cu): gathers per second.
-double measure_gather_rate(int64_t nnz, int32_t m, int32_t repeats);
 
 // The pump's constraint check on the device (checker.cu).
 struct Checker;

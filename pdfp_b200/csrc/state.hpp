@@ -31,10 +31,12 @@ struct InstState {
     double eps_opt, eps_feas, time_limit, omega;
     double art, suff, nec, kp, ki, kd, ismooth;
     double best_score;  // mixed precision: best KKT score seen (stall test)
+    double fp32_floor;  // mixed precision: relative residual the FP32 phase aims for
     int64_t inner, total, iter_limit;
+    int64_t fp64_iters;  // PDHG iterations of this solve run in FP64
     uint64_t t_start_ns;
     int32_t status, do_restart, restart_now, restarts;
-    int32_t freq, mode, stall, polish_windows;
+    int32_t freq, mode, stall, stall_limit;  // stall_limit: evaluations without progress before the polish (0: never)
     int32_t nnz_zero, pad0, pad1, pad2;
 };
 
@@ -43,8 +45,10 @@ struct SolveParams {
     double eps_opt, eps_feas, time_limit, omega;
     double art, suff, nec, kp, ki, kd, ismooth;
     double primal_weight;
+    double fp32_floor;
     int64_t iter_limit;
     int32_t freq, mode;
+    int32_t stall_limit, pad;
 };
 
 // What the host polls after every window.

@@ -70,6 +70,13 @@ def _out(out, size):
     return out
 
 
+def selftest_bounded_wait(which: int, limit_seconds: float = 0.05) -> int:
+    """Run the library's bounded-wait self-test (pdfp_selftest_bounded_wait): 0 the
+    mbarrier wait, 1 the grid barrier.  Returns the status code (E_TIMEOUT when the
+    wait gave up as designed)."""
+    return L.lib().pdfp_selftest_bounded_wait(int(which), float(limit_seconds))
+
+
 def set_device(device: int) -> None:
     """Select the CUDA device of this thread's later library calls (one per rank)."""
     L.check(L.lib().pdfp_set_device(int(device)))
@@ -115,6 +122,16 @@ class PDFPState:
                                     L.dptr(ub), L.dptr(w), L.dptr(ru), self._precision_code,
                                     C.byref(self._h)))
         self._created = True
+        if getattr(self, "_polish", None) is not None:
+            L.check(L.lib().pdfp_set_polish(self._h, *self._polish))
+
+    def set_polish(self, stall_evaluations: int = 10, fp32_floor: float = 1e-6):
+        """Mixed precision: when the FP64 polish takes over from the FP32 phase
+        (pdfp_set_polish): after `stall_evaluations` evaluations without a 10% KKT
+        improvement (0: never), or once the residuals reach `fp32_floor` under a
+        tighter tolerance."""
+        self._polish = (int(stall_evaluations), float(fp32_floor))
+        L.check(L.lib().pdfp_set_polish(self._h, *self._polish))
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -2,7 +2,7 @@
 
 Run in a container where the reference is mounted (it is not on the GPU box):
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <path of the reference checkout>
 
 It converts the reference's four example models (examples/*.mps.gz, the
 MIPLIB 2017 instances the reference's own tests use, test/runtests.jl:30-79)
@@ -56,4 +56,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <path of the reference checkout>")
+    main(sys.argv[1])

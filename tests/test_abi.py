@@ -78,12 +78,32 @@ def test_null_arguments_are_rejected_without_touching_the_device():
     assert b"null" in L.lib().pdfp_last_error()
     assert L.lib().pdfp_set_target(None, 0, None) == L.E_INVALID
     assert L.lib().pdfp_solve(None, None, 1.0, None) == L.E_INVALID
-    assert L.lib().pdfp_measure_gather_rate(1024, 100, 1, None) == L.E_INVALID
+
+
+def bench_lib():
+    """libpdfp_bench.so: the benchmark's gather-ceiling probe, outside the solver library."""
+    lib = C.CDLL(os.path.join(ROOT, "pdfp_b200", "lib", "libpdfp_bench.so"))
+    lib.pdfp_measure_gather_rate.argtypes = [C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+    lib.pdfp_bench_last_error.restype = C.c_char_p
+    return lib
+
+
+def test_gather_probe_lives_outside_the_solver_library():
+    assert not hasattr(C.CDLL(L.LIB_PATH), "pdfp_measure_gather_rate")
+    text = open(os.path.join(ROOT, "include", "pdfp_bench.h")).read()
+    syms = set(re.findall(r"PDFP_API\s+[\w\s\*]+?\b(pdfp_\w+)\s*\(", text))
+    lib = bench_lib()
+    assert syms == {"pdfp_measure_gather_rate", "pdfp_bench_last_error"}
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert lib.pdfp_measure_gather_rate(1024, 100, 1, None) == L.E_INVALID
+    assert b"null output" in lib.pdfp_bench_last_error()
 
 
 @pytest.mark.gpu
 def test_gather_rate_probe_reports_a_plausible_rate():
+    lib = bench_lib()
     r = C.c_double()
-    L.check(L.lib().pdfp_measure_gather_rate(4_000_000, 1_000_000, 3, C.byref(r)))
+    assert lib.pdfp_measure_gather_rate(4_000_000, 1_000_000, 3, C.byref(r)) == L.OK
     assert 1e10 < r.value < 1e13  # gathers per second
-    assert L.lib().pdfp_measure_gather_rate(1023, 100, 1, C.byref(r)) == L.E_INVALID
+    assert lib.pdfp_measure_gather_rate(1023, 100, 1, C.byref(r)) == L.E_INVALID

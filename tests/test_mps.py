@@ -11,10 +11,8 @@ import os
 import numpy as np
 import pytest
 
-from conftest import EXAMPLES, load_example
+from conftest import EXAMPLES, REF_EXAMPLES, load_example
 from pdfp_b200.milp import read_mps, read_mps_native
-
-REF_EXAMPLES = "/root/reference/examples"
 
 
 def same_model(a, b):
@@ -77,7 +75,8 @@ def test_native_equals_python_on_fixture_models(tmp_path, name):
     same_model(read_mps_native(p), read_mps(p))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
+@pytest.mark.skipif(not (REF_EXAMPLES and os.path.isdir(REF_EXAMPLES)),
+                    reason="no reference checkout (PDFP_REFERENCE_DIR)")
 @pytest.mark.parametrize("name", EXAMPLES)
 def test_native_equals_python_on_reference_examples(name):
     p = os.path.join(REF_EXAMPLES, f"{name}.mps.gz")

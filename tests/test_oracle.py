@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 import scipy.sparse as sp
 
-from conftest import GOLDEN
+from conftest import GOLDEN, REF_EXAMPLES
 from pdfp_b200.milp import MILP, is_feasible, num_continuous
 
 
@@ -45,12 +45,13 @@ def test_mps_reader_sizes(examples):
     assert num_continuous(examples["pk1"]) == 31
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/examples"), reason="reference tree absent")
+@pytest.mark.skipif(not (REF_EXAMPLES and os.path.isdir(REF_EXAMPLES)),
+                    reason="no reference checkout (PDFP_REFERENCE_DIR)")
 def test_mps_reader_matches_fixtures():
     from pdfp_b200.milp import read_mps
     from conftest import load_example
     for name in ["p0201", "pk1"]:
-        a = read_mps(f"/root/reference/examples/{name}.mps.gz")
+        a = read_mps(os.path.join(REF_EXAMPLES, f"{name}.mps.gz"))
         b = load_example(name)
         assert (a.A != b.A).nnz == 0 and np.array_equal(a.b, b.b) and np.array_equal(a.int_idx, b.int_idx)
 

@@ -10,6 +10,10 @@ ABI twice in a row, and checks both results against the allocating entry
 point pdfp_estimate_max_singular_value (same algorithm, start vector and
 summation order; estimates within 1e-10 relative, equal iteration counts).
 
+It also checks that a call made after the first on a device changes neither
+the device's free memory nor torch's allocator, runs a case near the scratch
+limit (few iterations), and checks the host-side rejections.
+
 This file sorts last so that a run stopping at the first failure has run
 every other test before it.
 """
@@ -35,21 +39,32 @@ def _device_csr(A):
     return rp, ci, v
 
 
-def _noalloc(A, max_iterations=5000, tolerance=1e-4):
+def _ptr(t, ty):
+    return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ty))
+
+
+def _noalloc_on(m, n, a, at, max_iterations=5000, tolerance=1e-4):
+    """One call of the entry point on device arrays a = (rp, ci, v) of A and at of A'."""
     import torch
-    m, n = A.shape
-    a = _device_csr(A)
-    at = _device_csr(sp.csr_matrix(A).T.tocsr())
-    ptr = lambda t, ty: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ty))  # noqa: E731
     sigma = C.c_double()
     its = C.c_int32()
     torch.cuda.synchronize()
     rc = L.lib().pdfp_estimate_max_singular_value_noalloc(
-        m, n, ptr(a[0], C.c_int32), ptr(a[1], C.c_int32), ptr(a[2], C.c_double),
-        ptr(at[0], C.c_int32), ptr(at[1], C.c_int32), ptr(at[2], C.c_double),
+        m, n, _ptr(a[0], C.c_int32), _ptr(a[1], C.c_int32), _ptr(a[2], C.c_double),
+        _ptr(at[0], C.c_int32), _ptr(at[1], C.c_int32), _ptr(at[2], C.c_double),
         max_iterations, tolerance, None, C.byref(sigma), C.byref(its))
     L.check(rc)
     return sigma.value, its.value
+
+
+def _device_pair(A):
+    return _device_csr(A), _device_csr(sp.csr_matrix(A).T.tocsr())
+
+
+def _noalloc(A, max_iterations=5000, tolerance=1e-4):
+    m, n = A.shape
+    a, at = _device_pair(A)
+    return _noalloc_on(m, n, a, at, max_iterations, tolerance)
 
 
 def _matrices():
@@ -77,3 +92,53 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
         600_000, 10, None, None, None, None, None, None, 10, 1e-4, None, C.byref(sigma), None)
     assert rc == L.E_UNSUPPORTED
     assert b"8 MiB" in L.lib().pdfp_last_error()
+
+
+def test_noalloc_second_call_allocates_nothing():
+    """After the first call on the device (which may commit the module's memory),
+    a call leaves the device's free memory and torch's allocator unchanged."""
+    import torch
+    A = _matrices()[1]
+    m, n = A.shape
+    a, at = _device_pair(A)
+    _noalloc_on(m, n, a, at)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    reserved0 = torch.cuda.memory_reserved()
+    s, it = _noalloc_on(m, n, a, at)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
+    assert torch.cuda.memory_reserved() == reserved0
+    ref, ref_it = gpu.estimate_max_singular_value(A)
+    assert s == pytest.approx(ref, rel=1e-10) and it == ref_it
+
+
+def test_noalloc_near_its_size_limit():
+    """2m + n + 2 = 1,047,002 of the 1,048,576 scratch values (the offsets of all three
+    work vectors and the result near the end of the array), three iterations."""
+    rng = np.random.default_rng(9)
+    m, n = 349_000, 349_000
+    A = sp.random(m, n, density=2.0 / n, random_state=rng, format="csr")
+    ref, ref_it = gpu.estimate_max_singular_value(A, max_iterations=3)
+    for _ in range(2):
+        s, it = _noalloc(A, max_iterations=3)
+        assert s == pytest.approx(ref, rel=1e-10)
+        assert it == ref_it == 3
+
+
+def test_noalloc_rejects_null_matrix_arrays():
+    import torch
+    A = _matrices()[0]
+    m, n = A.shape
+    a, at = _device_pair(A)
+    sigma = C.c_double()
+    torch.cuda.synchronize()
+    rc = L.lib().pdfp_estimate_max_singular_value_noalloc(
+        m, n, _ptr(a[0], C.c_int32), None, _ptr(a[2], C.c_double),
+        _ptr(at[0], C.c_int32), _ptr(at[1], C.c_int32), _ptr(at[2], C.c_double),
+        10, 1e-4, None, C.byref(sigma), None)
+    assert rc == L.E_INVALID
+    assert b"null matrix array" in L.lib().pdfp_last_error()
