@@ -693,6 +693,12 @@ def pump_bench(args, world, rank, embed=False):
     seeds = [s for s in range(1, 33) if (s - 1) % world == rank]
     arms = {"mixed_batched": [], "fp64_batched": [], "fp64_plain": []}
     found = {k: 0 for k in arms}
+    split = {k: [] for k in arms}  # (root LP, projections, rounding, pump iterations, PDHG iterations)
+
+    def note(k, r, dt):
+        arms[k].append(dt)
+        split[k].append((r.root_lp_time, r.projection_time, r.rounding_time, r.iterations,
+                         r.pdhg_iterations))
     warm = gen(1000)
     for _ in range(args.warmup):
         feasibility_pump_batched(warm, seeds=(101, 201), precision="mixed", time_limit=60)
@@ -701,37 +707,50 @@ def pump_bench(args, world, rank, embed=False):
         m = gen(s)
         t = time.perf_counter()
         r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="mixed", time_limit=60)
-        arms["mixed_batched"].append(time.perf_counter() - t)
+        note("mixed_batched", r, time.perf_counter() - t)
         found["mixed_batched"] += int(r.found and is_feasible(m, r.x))
         t = time.perf_counter()
         r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="fp64", time_limit=60)
-        arms["fp64_batched"].append(time.perf_counter() - t)
+        note("fp64_batched", r, time.perf_counter() - t)
         found["fp64_batched"] += int(r.found and is_feasible(m, r.x))
         t = time.perf_counter()
         r = feasibility_pump(m, seed=101, precision="fp64", time_limit=60)
-        arms["fp64_plain"].append(time.perf_counter() - t)
+        note("fp64_plain", r, time.perf_counter() - t)
         found["fp64_plain"] += int(r.found and is_feasible(m, r.x))
     if world > 1:
         import torch.distributed as dist
         gathered = [None] * world
-        dist.all_gather_object(gathered, (arms, found))
+        dist.all_gather_object(gathered, (arms, found, split))
         arms = {k: sum((g[0][k] for g in gathered), []) for k in arms}
         found = {k: sum(g[1][k] for g in gathered) for k in found}
+        split = {k: sum((g[2][k] for g in gathered), []) for k in split}
     if rank != 0:
         return
 
     def pct(v, q):
         return round(1e3 * float(np.percentile(v, q)), 2)
 
-    out = {k: {"p50_ms": pct(v, 50), "p90_ms": pct(v, 90), "found": found[k], "runs": len(v)}
+    def med_split(rows, total):
+        a = np.array(rows, dtype=np.float64)
+        root, proj, rnd = (round(1e3 * float(np.median(a[:, i])), 2) for i in range(3))
+        return {"root_lp_ms": root, "projection_ms": proj, "rounding_ms": rnd,
+                "other_host_ms": round(1e3 * float(np.median(np.asarray(total) - a[:, 0] - a[:, 1]
+                                                              - a[:, 2])), 2),
+                "pump_iterations": float(np.median(a[:, 3])),
+                "pdhg_iterations": float(np.median(a[:, 4]))}
+
+    out = {k: {"p50_ms": pct(v, 50), "p90_ms": pct(v, 90), "found": found[k], "runs": len(v),
+               "median_split": med_split(split[k], v)}
            for k, v in arms.items()}
     from oracle import oracle as O
-    cpu = []
+    cpu, cpu_split = [], []
     for s in range(1, 9):
         m = gen(s)
         t = time.perf_counter()
-        feasibility_pump_batched(m, seeds=(101, 201), solvers=O.OracleSolvers(), time_limit=60)
+        r, _ = feasibility_pump_batched(m, seeds=(101, 201), solvers=O.OracleSolvers(), time_limit=60)
         cpu.append(time.perf_counter() - t)
+        cpu_split.append((r.root_lp_time, r.projection_time, r.rounding_time, r.iterations,
+                          r.pdhg_iterations))
     line = {"metric": "time to first feasible, pump with 2 batched trajectories",
             "value": out["mixed_batched"]["p50_ms"], "unit": "ms (p50)", "n_gpus": world,
             "steps": len(arms["mixed_batched"]), "warmup": args.warmup,
@@ -743,7 +762,8 @@ def pump_bench(args, world, rank, embed=False):
                                                / max(out["mixed_batched"]["p90_ms"], 1e-9), 3),
             "cpu_baseline": {"value": round(1e3 * float(np.median(cpu)), 2), "unit": "ms (p50)",
                              "cores": 1, "kind": "port",
-                             "sample": "the same batched pump on the CPU oracle, model seeds 1..8"}}
+                             "sample": "the same batched pump on the CPU oracle, model seeds 1..8",
+                             "median_split": med_split(cpu_split, cpu)}}
     if embed:
         return line
     print(json.dumps(line), flush=True)
