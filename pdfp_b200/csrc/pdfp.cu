@@ -261,6 +261,81 @@ struct WarmStartCopy {  // initial = current (src/pdfp.jl:105-107)
     }
 };
 
+// ---- a small member's whole solve in one launch -------------------------------------
+//
+// For members of a few thousand rows and columns every launch and every host poll
+// costs more than the work of a window.  tiny_solve_kernel runs whole evaluation
+// windows of pdfp_solve! (src/pdfp.jl:258-285) for member blockIdx.x in one block:
+// step 1, the evaluation after a restart, steps 2 .. freq-1, step freq, the full
+// evaluation, the controller (termination, should_restart, PID) and the restart copy,
+// window after window, until the member stops, asks for the FP64 polish, or
+// max_windows windows have run.  The passes are tiny_pass (the one-block steps) and
+// tiny_eval_pass; the controller is the window's own (Controller::finalize), on the
+// block-summed terms.
+constexpr int kTinyWindowsPerLaunch = 64;
+
+template <typename T>
+__global__ void __launch_bounds__(kTinyThreads)
+    tiny_solve_kernel(IterVecs<T> v, EvalData ed, InstState* st, InstFlags* fl,
+                      const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
+                      const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
+                      const int32_t* __restrict__ col_off, const int32_t* __restrict__ row_off,
+                      const int32_t* __restrict__ n_eq, int32_t* err, int32_t max_windows,
+                      int32_t polish) {
+    constexpr int NT = kTinyThreads;
+    constexpr int32_t mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    extern __shared__ __align__(16) double tiny_rowsum[];  // 2 * max(rows, columns) of a member
+    __shared__ double red[8 * (NT / 32)];
+    __shared__ int32_t go;
+    const int p = blockIdx.x;
+    const int32_t c0 = col_off[p], c1 = col_off[p + 1], r0 = row_off[p], r1 = row_off[p + 1];
+    // the evaluation terms of one phase, block-summed, then the controller (thread 0)
+    auto evaluate = [&](int32_t which, int32_t phase) {
+        double ac[8], ar[4];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) ac[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ar[k] = 0.0;
+        tiny_eval_pass(EvalColOp<T, NT>{v, ed, st, which, mode, err}, rp_t, ci_t, c0, c1, p, tiny_rowsum, ac);
+        block_sum<NT, 8>(ac, red, threadIdx.x);
+        tiny_eval_pass(EvalRowOp<T, NT>{v, ed, st, row_off, n_eq, which, mode, err}, rp_a, ci_a, r0, r1, p,
+                       tiny_rowsum, ar);
+        block_sum<NT, 4>(ar, red, threadIdx.x);
+        if (threadIdx.x == 0) {
+            const double a[12] = {ac[0], ac[1], ac[2], ac[3], ac[4], ac[5], ac[6], ac[7],
+                                  ar[0], ar[1], ar[2], ar[3]};
+            Controller{nullptr, nullptr, nullptr, nullptr, st, fl, phase, polish}.finalize(p, a);
+        }
+        __syncthreads();
+    };
+    for (int32_t w = 0; w < max_windows; ++w) {
+        if (threadIdx.x == 0) go = st[p].status == ST_RUNNING && st[p].mode == mode;
+        __syncthreads();
+        if (!go) break;
+        const int32_t freq = st[p].freq;
+        for (int32_t i = 1; i <= freq; ++i) {
+            if (i == 1 || i == freq) {  // major steps: pdhg_* and reflected_* are read after them
+                tiny_pass(PrimalOp<T, true, NT>{v, st, i, mode, err, 0}, rp_t, ci_t, c0, c1, p);
+                __syncthreads();
+                tiny_pass(DualOp<T, true, NT>{v, st, row_off, n_eq, i, mode, err, 0}, rp_a, ci_a, r0, r1, p);
+            } else {
+                tiny_pass(PrimalOp<T, false, NT>{v, st, i, mode, err, 0}, rp_t, ci_t, c0, c1, p);
+                __syncthreads();
+                tiny_pass(DualOp<T, false, NT>{v, st, row_off, n_eq, i, mode, err, 0}, rp_a, ci_a, r0, r1, p);
+            }
+            __syncthreads();
+            if (i == 1 && st[p].do_restart) evaluate(EVAL_AFTER_RESTART, PHASE_AFTER_FIRST);
+        }
+        evaluate(EVAL_FULL, PHASE_EVAL);
+        const RestartCopy<T> rc{v, st, col_off, row_off, mode};
+        if (rc.active(p))
+            for (int32_t i = threadIdx.x; i < (c1 - c0) + (r1 - r0); i += NT) rc.elem(p, i);
+        if (threadIdx.x == 0) go = st[p].status == ST_RUNNING && !fl[p].polish_request;
+        __syncthreads();
+        if (!go) break;
+    }
+}
+
 // dst[packed j] = src[caller index of j] for instance `only` (columns or rows)
 template <typename T>
 struct PermuteIn {
@@ -1216,15 +1291,30 @@ void Projector::prepare_window() {
     g_.er = tile_grid<EvalRowOp<double, NT_EVAL>>(ev_a_.dev, num_sms_);
 }
 
-// One evaluation window on the stream: a small handle's window (a dozen launches)
-// is issued directly; any other replays the window's captured graph.
+// Evaluation windows on the stream: a small handle runs up to kTinyWindowsPerLaunch
+// windows of every member in one launch per precision (tiny_solve_kernel); any other
+// handle replays one window's captured graph.
 void Projector::run_window(int freq, bool with32, bool with64) {
     if (tiny_ && !timing_) {
+        const size_t smem = sizeof(double) * 2 * static_cast<size_t>(std::max(M_.max_m, M_.max_n));
         if (!window_ready_) {
-            prepare_window();
+            if (smem > 48 * 1024) {
+                PDFP_CK(cudaFuncSetAttribute(tiny_solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+                PDFP_CK(cudaFuncSetAttribute(tiny_solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+            }
             window_ready_ = true;
         }
-        record_window(freq, with32, with64);
+        (void)freq;  // each member's own evaluation frequency (its state) drives the kernel
+        if (with32)
+            tiny_solve_kernel<float><<<K_, kTinyThreads, smem, stream_>>>(
+                v32_, ed_, st_, flags_, M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, M_.n_eq,
+                err_, kTinyWindowsPerLaunch, polish_enabled_);
+        if (with64)
+            tiny_solve_kernel<double><<<K_, kTinyThreads, smem, stream_>>>(
+                v64_, ed_, st_, flags_, M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, M_.n_eq,
+                err_, kTinyWindowsPerLaunch, polish_enabled_);
         PDFP_CK(cudaGetLastError());
         return;
     }

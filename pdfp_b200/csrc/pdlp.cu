@@ -238,6 +238,92 @@ struct LpRestartCopy {
     }
 };
 
+// ---- a small LP's whole solve in one launch ---------------------------------------------
+//
+// As for the projector (tiny_solve_kernel, pdfp.cu): one block runs whole evaluation
+// windows of pdlp_solve! (src/pdlp.jl:332-370) -- step 1, the evaluation after a
+// restart, steps 2 .. freq-1, step freq, the full evaluation, the cuPDLPx ray passes,
+// the controller and the restart copy -- until the LP stops, asks for the FP64 polish,
+// or max_windows windows have run.
+constexpr int kLpTinyWindowsPerLaunch = 64;
+
+template <typename T>
+__global__ void __launch_bounds__(kTinyThreads)
+    lp_tiny_solve_kernel(LpVecs<T> v, LpData d, InstState* st, InstFlags* fl,
+                         const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
+                         const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
+                         int32_t n, int32_t m, int32_t* err, int32_t cupdlpx, int32_t max_windows) {
+    constexpr int NT = kTinyThreads;
+    constexpr int32_t mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    extern __shared__ __align__(16) double lp_rowsum[];  // 2 * max(n, m)
+    __shared__ double red[8 * (NT / 32)];
+    __shared__ int32_t go;
+    auto evaluate = [&](int32_t which, int32_t phase) {
+        double ac[8], ar[4];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) ac[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ar[k] = 0.0;
+        tiny_eval_pass(LpEvalColOp<T, NT>{v, d, st, which, mode, err}, rp_t, ci_t, 0, n, 0, lp_rowsum, ac);
+        block_sum<NT, 8>(ac, red, threadIdx.x);
+        tiny_eval_pass(LpEvalRowOp<T, NT>{v, d, st, which, mode, err}, rp_a, ci_a, 0, m, 0, lp_rowsum, ar);
+        block_sum<NT, 4>(ar, red, threadIdx.x);
+        if (phase == 1 && cupdlpx) {  // compute_infeasibility_information!, src/pdlp.jl:247-285
+            if (threadIdx.x < 4) d.maxes[threadIdx.x] = 0ull;
+            __syncthreads();
+            double none[2] = {0.0, 0.0};
+            const RayRowsCol<T> rc{v, d, st};
+            for (int32_t j = threadIdx.x; j < n; j += NT) rc.row(j, 0, none);
+            double rr[1] = {0.0};
+            const RayRowsRow<T> rw{v, d, st, nullptr};
+            for (int32_t i = threadIdx.x; i < m; i += NT) rw.row(i, 0, rr);
+            block_sum<NT, 1>(rr, red, threadIdx.x);  // its barriers also order dray, yray and the maxima
+            double a2[2] = {0.0, 0.0};
+            tiny_eval_pass(RayColOp<NT>{d, st, nullptr, err}, rp_t, ci_t, 0, n, 0, lp_rowsum, a2);
+            block_sum<NT, 2>(a2, red, threadIdx.x);
+            double a0[1] = {0.0};
+            tiny_eval_pass(RayRowOp<NT>{d, st, err}, rp_a, ci_a, 0, m, 0, lp_rowsum, a0);
+            if (threadIdx.x == 0) {
+                const double a[3] = {a2[0], a2[1], rr[0]};
+                LpRayFin{nullptr, nullptr, nullptr, nullptr, st, d.maxes}.finalize(0, a);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const double a[12] = {ac[0], ac[1], ac[2], ac[3], ac[4], ac[5], ac[6], ac[7],
+                                  ar[0], ar[1], ar[2], ar[3]};
+            LpController{nullptr, nullptr, nullptr, nullptr, st, fl, phase, cupdlpx}.finalize(0, a);
+        }
+        __syncthreads();
+    };
+    for (int32_t w = 0; w < max_windows; ++w) {
+        if (threadIdx.x == 0) go = st[0].status == ST_RUNNING && st[0].mode == mode;
+        __syncthreads();
+        if (!go) break;
+        const int32_t freq = st[0].freq;
+        for (int32_t i = 1; i <= freq; ++i) {  // pdhg_step!, src/pdlp.jl:147-153
+            if (i == 1 || i == freq) {
+                tiny_pass(LpPrimalOp<T, true, NT>{v, st, i, mode, err}, rp_t, ci_t, 0, n, 0);
+                __syncthreads();
+                tiny_pass(LpDualOp<T, true, NT>{v, st, i, mode, err}, rp_a, ci_a, 0, m, 0);
+            } else {
+                tiny_pass(LpPrimalOp<T, false, NT>{v, st, i, mode, err}, rp_t, ci_t, 0, n, 0);
+                __syncthreads();
+                tiny_pass(LpDualOp<T, false, NT>{v, st, i, mode, err}, rp_a, ci_a, 0, m, 0);
+            }
+            __syncthreads();
+            if (i == 1 && st[0].do_restart) evaluate(EVAL_AFTER_RESTART, 0);
+        }
+        evaluate(EVAL_FULL, 1);
+        const LpRestartCopy<T> rc{v, st, n, m};
+        if (rc.active(0))
+            for (int32_t i = threadIdx.x; i < n + m; i += NT) rc.elem(0, i);
+        if (threadIdx.x == 0) go = st[0].status == ST_RUNNING && !fl[0].polish_request;
+        __syncthreads();
+        if (!go) break;
+    }
+}
+
 __global__ void lp_begin_kernel(InstState* st) { st[0].t_start_ns = globaltimer_ns(); }
 __global__ void zero_maxes_kernel(unsigned long long* m) {
     if (threadIdx.x < 4) m[threadIdx.x] = 0ull;
@@ -378,10 +464,12 @@ class LpSolver {
     template <typename T>
     void record(int freq);
     template <typename T>
+    void launch_tiny_solve();
+    template <typename T>
     void prepare_grids();
 
     bool cupdlpx_, f32_;
-    bool tiny_ = false;  // small LP: a window's minor steps in one launch
+    bool tiny_ = false;  // small LP: whole windows in one launch (lp_tiny_solve_kernel)
     int sms_ = 148;
     int32_t m_ = 0, n_ = 0;
     cudaStream_t stream_ = nullptr;
@@ -475,6 +563,21 @@ void LpSolver::record(int freq) {
     launch_elem(1, static_cast<int64_t>(n_) + m_, LpRestartCopy<T>{v, st_, n_, m_}, stream_);
 }
 
+// A small LP: up to kLpTinyWindowsPerLaunch windows in one launch (lp_tiny_solve_kernel).
+template <typename T>
+void LpSolver::launch_tiny_solve() {
+    LpVecs<T>* vp = nullptr;
+    if constexpr (std::is_same<T, float>::value) vp = &v32_; else vp = &v64_;
+    const size_t smem = sizeof(double) * 2 * static_cast<size_t>(std::max(std::max(n_, m_), 1));
+    if (smem > 48 * 1024)
+        PDFP_CK(cudaFuncSetAttribute(lp_tiny_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+    lp_tiny_solve_kernel<T><<<1, kTinyThreads, smem, stream_>>>(*vp, d_, st_, flags_, M_.rp_t, M_.ci_t,
+                                                                M_.rp_a, M_.ci_a, n_, m_, err_,
+                                                                cupdlpx_ ? 1 : 0, kLpTinyWindowsPerLaunch);
+    PDFP_CK(cudaGetLastError());
+}
+
 template <typename T>
 cudaGraphExec_t LpSolver::build_graph(int freq) {
     prepare_grids<T>();
@@ -541,15 +644,12 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
     // capture and instantiate per solve; a larger one replays a captured window
     bool f32_window = f32_;
     if (!tiny_) graph_ = f32_ ? build_graph<float>(200) : build_graph<double>(200);
-    else if (f32_) prepare_grids<float>();
-    else prepare_grids<double>();
 
     InstFlags fh[2] = {};  // a few bytes per poll: pageable memory, no page-locked allocation
     {
         for (;;) {
             if (tiny_) {
-                if (f32_window) record<float>(200); else record<double>(200);
-                PDFP_CK(cudaGetLastError());
+                if (f32_window) launch_tiny_solve<float>(); else launch_tiny_solve<double>();
             } else {
                 PDFP_CK(cudaGraphLaunch(graph_, stream_));
             }
@@ -564,7 +664,7 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
                 PDFP_CK(cudaGetLastError());
                 if (graph_) cudaGraphExecDestroy(graph_);
                 graph_ = nullptr;
-                if (tiny_) prepare_grids<double>(); else graph_ = build_graph<double>(200);
+                if (!tiny_) graph_ = build_graph<double>(200);
                 f32_window = false;
                 polished_ = true;
             }

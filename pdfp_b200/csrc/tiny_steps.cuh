@@ -71,6 +71,59 @@ __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restric
     }
 }
 
+// One evaluation pass of instance `inst` over rows [r0, r1), in one block: each row's
+// NV sums of products (G lanes per row, as tiny_pass) go to shared memory
+// (rowsum[q * R + rr]), then the Op's per-row terms accumulate into acc with row rr on
+// thread rr % NTH -- the tile engine epilogue's assignment -- so that the block sum
+// that follows adds them in the same order as a one-tile evaluation launch.
+template <class Op, int NTH = kTinyThreads>
+__device__ __forceinline__ void tiny_eval_pass(const Op& op, const int32_t* __restrict__ rp,
+                                               const int32_t* __restrict__ ci, int32_t r0,
+                                               int32_t r1, int inst, typename Op::AT* rowsum,
+                                               double* acc) {
+    using AT = typename Op::AT;
+    using GT = typename Op::GT;
+    constexpr int NV = Op::NV;
+    const auto* vals = op.values();
+    const int32_t R = r1 - r0;
+    int G = 1;
+    while (G < 32 && G * 2 * R <= NTH) G *= 2;
+    const int groups = NTH / G;
+    const int gid = threadIdx.x / G, lane = threadIdx.x & (G - 1);
+    for (int32_t b = 0; b < R; b += groups) {
+        const int32_t rr = b + gid;
+        AT s[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) s[q] = AT(0);
+        if (rr < R) {
+            const int32_t row = r0 + rr;
+            for (int32_t k = rp[row] + lane; k < rp[row + 1]; k += G) {
+                GT g[NV];
+                op.gather(ci[k], g);
+                const AT a = static_cast<AT>(vals[k]);
+#pragma unroll
+                for (int q = 0; q < NV; ++q) s[q] = add_rn(s[q], mul_rn(a, static_cast<AT>(g[q])));
+            }
+        }
+        for (int o = G >> 1; o > 0; o >>= 1)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) s[q] = add_rn(s[q], __shfl_xor_sync(0xffffffffu, s[q], o));
+        if (rr < R && lane == 0)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) rowsum[q * R + rr] = s[q];
+    }
+    __syncthreads();
+    const typename Op::TileP tp = op.tile_params(inst);
+    const typename Op::VT* none[1] = {nullptr};
+    for (int32_t rr = threadIdx.x; rr < R; rr += NTH) {
+        AT sums[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sums[q] = rowsum[q * R + rr];
+        op.row(r0 + rr, rr, inst, tp, none, sums, acc);
+    }
+    __syncthreads();  // rowsum is reused by the next pass
+}
+
 // Steps i0 .. i1-1 (minor: no pdhg_* / reflected_* outputs) of instance blockIdx.x:
 // POp runs on the rows of A' (columns), DOp on the rows of A; both carry the step
 // index in k_offset.
