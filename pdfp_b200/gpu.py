@@ -203,6 +203,14 @@ class PDFPState:
         L.check(L.lib().pdfp_get_vector_unscaled(self._h, 0, L.VEC[which], L.dptr(out)))
         return out[:self.n]
 
+    def tuning(self):
+        """The step kernels' configuration (pdfp_get_tuning): A' stage bytes, threads,
+        tiles, A stage bytes, threads, tiles, A' gather policy, A gather policy (3: the
+        segmented engine)."""
+        out = (C.c_int32 * 8)()
+        L.check(L.lib().pdfp_get_tuning(self._h, out))
+        return list(out)
+
     def profile_step(self, iterations: int):
         a, b = C.c_float(), C.c_float()
         ba, bb = C.c_double(), C.c_double()
