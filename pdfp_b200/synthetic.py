@@ -74,20 +74,26 @@ def _sorted_unique(key: np.ndarray) -> np.ndarray:
     return key[keep]
 
 
-def _rows_with_lengths(rng, lengths: np.ndarray, n: int):
-    """Row index / distinct column index arrays for the given row lengths."""
+def _rows_with_lengths(rng, lengths: np.ndarray, n: int, band: int = 0):
+    """Row index / distinct column index arrays for the given row lengths.  band > 0 draws
+    row i's columns within +-band of its diagonal position i * n / m (wrapping)."""
     m = len(lengths)
     total = int(lengths.sum())
     rows = np.repeat(np.arange(m, dtype=np.int64), lengths)
-    cols = rng.integers(0, n, size=total, dtype=np.int64)
+
+    def draw(r):
+        if band <= 0:
+            return rng.integers(0, n, size=len(r), dtype=np.int64)
+        return (r * n // m + rng.integers(-band, band + 1, size=len(r), dtype=np.int64)) % n
+
+    cols = draw(rows)
     # make columns distinct within each row: sort, drop repeats, top up with fresh draws
     key = rows * n + cols
     key = _sorted_unique(key)
     missing = total - len(key)
     while missing > 0:
         extra_rows = rng.integers(0, m, size=missing, dtype=np.int64)
-        extra_cols = rng.integers(0, n, size=missing, dtype=np.int64)
-        key = _sorted_unique(np.concatenate([key, extra_rows * n + extra_cols]))
+        key = _sorted_unique(np.concatenate([key, extra_rows * n + draw(extra_rows)]))
         missing = total - len(key)
     return key // n, key % n
 
@@ -150,15 +156,20 @@ def zipf_lengths(rng, m: int, nnz: int, a: float = 1.5, cap: int = 10000) -> np.
     return L
 
 
-def zipf_lp(seed: int = 1, m: int = 1_000_000, n: int = 2_000_000, nnz: int = 20_000_000):
+def zipf_lp(seed: int = 1, m: int = 1_000_000, n: int = 2_000_000, nnz: int = 20_000_000,
+            band: int = 0):
     """LP relaxation for the bandwidth stress: n columns (first half binary, second half
     continuous in [0, 1]), Zipf(1.5) row lengths capped at 10,000 and rescaled to exactly `nnz`
     nonzeros, U[-1, 1] values, <= rows with b = A x_f + U[0, 1] for a random point x_f.
+    band > 0: a variant with locality -- each row's columns within +-band of its diagonal
+    position (band is raised to the longest row so that every row fits).
     Returns (milp, x_f)."""
     rng = _rng(seed)
     lengths = zipf_lengths(rng, m, nnz)
     lengths = np.minimum(lengths, n)
-    rows, cols = _rows_with_lengths(rng, lengths, n)
+    if band > 0:
+        band = min(max(band, int(lengths.max())), n // 2)
+    rows, cols = _rows_with_lengths(rng, lengths, n, band)
     vals = rng.uniform(-1.0, 1.0, size=len(rows))
     A = _csr_from_keys(rows * n + cols, vals, m, n)
     n_bin = n // 2
