@@ -18,7 +18,15 @@ iterations over ranks / max time.
 
 --impl reference times the reference's own CPU algorithm (the C restatement
 under oracle/, every host thread) on a bounded sample of the same workload:
-each step runs a fixed number of PDHG iterations of the same projection.
+each step projects the next target of the same sequence with the whole
+pdfp_solve! loop (steps, evaluation windows, restart tests, PID), cut at
+--cpu-iterations iterations (one evaluation window by default).
+
+The default line also carries: the plain FP64 form on the same targets; the
+mixed form's error per projection (`parity`); the step kernels' rooflines;
+the same generator with a locality band (`zipf_lp_banded`); the batched
+uneven projections (`batch_uneven`, config 3) and the markshare-shaped pumps
+(`pump_markshare`, config 4); and a single-thread CPU baseline.
 """
 from __future__ import annotations
 
