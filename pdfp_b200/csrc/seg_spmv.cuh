@@ -38,8 +38,6 @@ namespace pdfp {
 constexpr int kSegQ = 8;          // CTAs per cluster (the portable cluster size)
 constexpr int kSegColBits = 17;   // column-in-segment bits of a key
 constexpr int kSegThreads = 512;  // threads per CTA
-constexpr int kSegU = 4;          // 32-nonzero windows in flight per warp
-constexpr uint32_t kSegNoKey = 0xFFFFFFFFu;  // past a chunk's end (no row reaches 2^15 - 1)
 
 // One side of the matrix in the segmented layout (device view).
 struct SegDev {
@@ -133,44 +131,31 @@ __global__ void __launch_bounds__(kSegThreads) seg_spmv_kernel(const SegDev s, c
         }
         const uint32_t base = smem_addr(xb[seg & 1]);
         const int32_t k0 = s.chunk_off[g * s.S + seg], k1 = s.chunk_off[g * s.S + seg + 1];
-        // a warp takes kSegU consecutive windows of 32 nonzeros at a time: every key and
-        // value load first, then every gather, then the scans -- kSegU independent chains
-        for (int32_t w0 = k0 + warp * 32 * kSegU; w0 < k1; w0 += NW * 32 * kSegU) {
-            uint32_t kk[kSegU];
-            float pv[kSegU];
-#pragma unroll
-            for (int u = 0; u < kSegU; ++u) {
-                const int32_t k = w0 + 32 * u + lane;
-                kk[u] = k < k1 ? __ldcs(s.key + k) : kSegNoKey;
-                pv[u] = k < k1 ? __ldcs(s.val + k) : 0.f;
+        for (int32_t w = k0 + warp * 32; w < k1; w += NW * 32) {
+            const int32_t k = w + lane;
+            const bool valid = k < k1;
+            const uint32_t kk = valid ? __ldcs(s.key + k) : 0xFFFFFFFFu;
+            float p = 0.f;
+            if (valid) {
+                const float a = __ldcs(s.val + k);
+                const uint32_t col = kk & ((1u << kSegColBits) - 1u);
+                p = mul_rn(a, ld_shared_cluster(map_shared_rank(base + 4u * (col & (SL - 1)), col >> SL_LOG)));
             }
+            // segmented inclusive scan over the lanes of each row's run (rows ascend)
+            const uint32_t row = kk >> kSegColBits;
 #pragma unroll
-            for (int u = 0; u < kSegU; ++u) {
-                const uint32_t col = kk[u] & ((1u << kSegColBits) - 1u);
-                if (kk[u] != kSegNoKey)
-                    pv[u] = mul_rn(pv[u], ld_shared_cluster(map_shared_rank(base + 4u * (col & (SL - 1)), col >> SL_LOG)));
+            for (int d = 1; d < 32; d <<= 1) {
+                const float t = __shfl_up_sync(0xffffffffu, p, d);
+                const uint32_t tr = __shfl_up_sync(0xffffffffu, row, d);
+                if (lane >= d && tr == row) p = add_rn(t, p);
             }
-#pragma unroll
-            for (int u = 0; u < kSegU; ++u) {
-                const int32_t w = w0 + 32 * u;
-                if (w >= k1) break;  // warp-uniform
-                // segmented inclusive scan over the lanes of each row's run (rows ascend)
-                const uint32_t row = kk[u] >> kSegColBits;
-                float p = pv[u];
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const float t = __shfl_up_sync(0xffffffffu, p, d);
-                    const uint32_t tr = __shfl_up_sync(0xffffffffu, row, d);
-                    if (lane >= d && tr == row) p = add_rn(t, p);
-                }
-                const uint32_t next = __shfl_down_sync(0xffffffffu, row, 1);
-                const uint32_t row0 = __shfl_sync(0xffffffffu, row, 0);
-                if (kk[u] != kSegNoKey && (lane == 31 || next != row)) {
-                    // the run of lane 0 continues a row of the previous window: a partial
-                    const bool cont = row == row0 && w > k0 && (__ldg(s.key + w - 1) >> kSegColBits) == row0;
-                    if (cont) side[(w - k0) >> 5] = p;
-                    else acc[row] = add_rn(acc[row], p);
-                }
+            const uint32_t next = __shfl_down_sync(0xffffffffu, row, 1);
+            const uint32_t row0 = __shfl_sync(0xffffffffu, row, 0);
+            if (valid && (lane == 31 || next != row)) {
+                // the run of lane 0 continues a row of the previous window: a partial
+                const bool cont = row == row0 && w > k0 && (__ldg(s.key + w - 1) >> kSegColBits) == row0;
+                if (cont) side[(w - k0) >> 5] = p;
+                else acc[row] = add_rn(acc[row], p);
             }
         }
         __syncthreads();
