@@ -176,56 +176,4 @@ std::string build_layout(const std::vector<ProblemIn>& probs, bool permute, Host
     return "";
 }
 
-std::string build_seg_layout(const HostCsr& C, int G, int q, int sl_log, SegHost& out) {
-    out = SegHost{};
-    const int64_t rows = C.rows, nnz = C.rp.empty() ? 0 : C.rp[rows];
-    if (rows == 0 || nnz == 0 || C.cols == 0) return "empty side";
-    if (G < q || G % q != 0) return "CTA count must be a positive multiple of the cluster size";
-    const int64_t seg = static_cast<int64_t>(q) << sl_log;
-    if (seg > (int64_t(1) << 17)) return "a segment is wider than a key's 17 column bits";
-    const int64_t S = (C.cols + seg - 1) / seg;
-    // contiguous row ranges balanced by nonzeros plus two per row (the epilogue)
-    const double total = static_cast<double>(nnz) + 2.0 * static_cast<double>(rows);
-    out.row_start.assign(G + 1, 0);
-    int64_t r = 0;
-    for (int g = 1; g < G; ++g) {
-        const double want = total * g / G;
-        while (r < rows && static_cast<double>(C.rp[r + 1]) + 2.0 * static_cast<double>(r + 1) <= want) ++r;
-        out.row_start[g] = static_cast<int32_t>(r);
-    }
-    out.row_start[G] = static_cast<int32_t>(rows);
-    int32_t rmax = 0;
-    for (int g = 0; g < G; ++g) rmax = std::max(rmax, out.row_start[g + 1] - out.row_start[g]);
-    if (rmax >= (1 << 15)) return "more than 32767 rows on one CTA";
-    std::vector<int64_t> cnt(static_cast<size_t>(G) * S, 0);
-    for (int g = 0; g < G; ++g)
-        for (int32_t i = out.row_start[g]; i < out.row_start[g + 1]; ++i)
-            for (int32_t k = C.rp[i]; k < C.rp[i + 1]; ++k) ++cnt[static_cast<size_t>(g) * S + C.ci[k] / seg];
-    out.chunk_off.assign(static_cast<size_t>(G) * S + 1, 0);
-    int64_t wmax = 0;
-    for (size_t c = 0; c < cnt.size(); ++c) {
-        out.chunk_off[c + 1] = static_cast<int32_t>(out.chunk_off[c] + cnt[c]);
-        wmax = std::max(wmax, (cnt[c] + 31) / 32);
-    }
-    std::vector<int64_t> pos(out.chunk_off.begin(), out.chunk_off.end() - 1);
-    out.key.resize(nnz);
-    out.val.resize(nnz);
-    for (int g = 0; g < G; ++g)
-        for (int32_t i = out.row_start[g]; i < out.row_start[g + 1]; ++i)
-            for (int32_t k = C.rp[i]; k < C.rp[i + 1]; ++k) {
-                const int64_t s = C.ci[k] / seg;
-                const int64_t p = pos[static_cast<size_t>(g) * S + s]++;
-                out.key[p] = (static_cast<uint32_t>(i - out.row_start[g]) << 17) |
-                             static_cast<uint32_t>(C.ci[k] - s * seg);
-                out.val[p] = static_cast<float>(C.v[k]);
-            }
-    out.G = G;
-    out.S = static_cast<int32_t>(S);
-    out.sl_log = sl_log;
-    out.rmax = rmax;
-    out.wmax = static_cast<int32_t>(std::max<int64_t>(wmax, 1));
-    out.ncols = C.cols;
-    return "";
-}
-
 }  // namespace pdfp

@@ -173,20 +173,4 @@ struct HostLayout {
 // ascending within rows); returns an error message or "" and fills `out`.
 std::string build_layout(const std::vector<ProblemIn>& probs, bool permute, HostLayout& out);
 
-// One side of the matrix for the segmented FP32 engine (seg_spmv.cuh): G CTAs in
-// clusters of q own contiguous row ranges balanced by nonzeros (at most 2^15 - 1
-// rows each); the columns are cut into segments of q << sl_log entries; the
-// nonzeros of CTA g in segment s are chunk g * S + s, each a key
-// (row in the CTA << 17 | column in the segment) and an FP32 value, sorted by row
-// and, within a row, in the CSR's (ascending) order.
-struct SegHost {
-    int32_t G = 0, S = 0, sl_log = 0, rmax = 0, wmax = 0, ncols = 0;
-    std::vector<int32_t> row_start, chunk_off;
-    std::vector<uint32_t> key;
-    std::vector<float> val;
-};
-// Returns "" or why the side does not fit the layout (too many rows per CTA, a
-// segment wider than a key holds, an empty side).
-std::string build_seg_layout(const HostCsr& C, int G, int q, int sl_log, SegHost& out);
-
 }  // namespace pdfp

@@ -672,17 +672,12 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     const char* se = std::getenv("PDFP_STEP_ENGINE");
     const int forced = !se ? -1
                        : std::strcmp(se, "tile") == 0 ? 0
-                       : std::strcmp(se, "flat") == 0 || std::strcmp(se, "flat1") == 0 ? 1
-                       : std::strcmp(se, "seg") == 0 ? 2 : -1;
+                       : std::strcmp(se, "flat") == 0 || std::strcmp(se, "flat1") == 0 ? 1 : -1;
     if (forced >= 0) {
         const int qpt = std::strcmp(se, "flat1") == 0 ? 1 : 2;
         for (StepSide* q : {&p32_, &d32_, &p64_, &d64_}) {
             q->engine = forced;
             q->qpt = qpt;
-        }
-        if (forced == 2) {  // FP32 sides only; the FP64 form keeps the tile engine
-            p64_.engine = d64_.engine = 0;
-            p32_.stage_bytes = d32_.stage_bytes = 64 * 1024;
         }
     }
     // PDFP_TUNING="s,t,l,s,t,l" pins both sides' step kernels of this precision
@@ -706,16 +701,6 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
             for (int f = 0; f < 2; ++f) {
                 StepSide& q = *sides[f][k];
                 const int* c = v + 3 * k;
-                if (c[2] == 3) {  // the segmented engine: slice bytes, kSegThreads threads
-                    if (c[1] != kSegThreads || (c[0] != 32768 && c[0] != 65536))
-                        throw Error(E_INVALID, "PDFP_TUNING: gather policy 3 (segmented engine) takes "
-                                               "32768 or 65536 slice bytes and 512 threads");
-                    q.engine = f == 0 ? 2 : 0;  // FP32 sides only
-                    q.stage_bytes = f == 0 ? c[0] : q.stage_bytes;
-                    q.nt = f == 0 ? kSegThreads : q.nt;
-                    q.gather_l2 = f == 0 ? 3 : 0;
-                    continue;
-                }
                 if (c[1] != 0 && c[1] != 128 && c[1] != 256)
                     throw Error(E_INVALID, "PDFP_TUNING: threads per role must be 0, 128 or 256");
                 if (c[1] != 0 && (c[0] < 8192 || c[0] > 49152 || c[0] % 128 != 0))
@@ -741,18 +726,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
                       : at && at[0] == '0' ? false
                       : (at && at[0] == '1' ? true : M_.L.NNZ >= (1 << 18));
     if (precision_ == PDFP_MIXED) {
-        if (tune) {
-            autotune(true);
-        } else {
-            for (int side = 0; side < 2; ++side) {
-                StepSide& q = side == 0 ? p32_ : d32_;
-                prepare_side(q, side == 0, true);
-                if (q.engine == 2 && q.grid <= 0) {  // does not fit the segmented layout
-                    q = StepSide{};
-                    prepare_side(q, side == 0, true);
-                }
-            }
-        }
+        if (tune) autotune(true); else { prepare_side(p32_, true, true); prepare_side(d32_, false, true); }
     }
     if (tune && precision_ == PDFP_FP64) {
         autotune(false);
@@ -767,36 +741,9 @@ IterVecs<float>& Projector::vecs<float>() { return v32_; }
 template <>
 IterVecs<double>& Projector::vecs<double>() { return v64_; }
 
-// A step pass on the segmented engine: a cluster launch of kSegQ CTAs per cluster.
-template <class Op>
-static void launch_seg(const SegDev& d, int sl_log, size_t smem, const Op& op, cudaStream_t stream) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(static_cast<unsigned>(d.G));
-    cfg.blockDim = dim3(kSegThreads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = stream;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kSegQ;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    if (sl_log == 14)
-        PDFP_CK(cudaLaunchKernelEx(&cfg, seg_spmv_kernel<Op, 14>, d, op));
-    else
-        PDFP_CK(cudaLaunchKernelEx(&cfg, seg_spmv_kernel<Op, 13>, d, op));
-}
-
 template <typename T, bool MAJOR>
 void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    if constexpr (std::is_same<T, float>::value) {
-        if (s.engine == 2) {
-            launch_seg(s.seg, s.sl_log, s.seg_smem, PrimalOp<float, MAJOR, 256>{vecs<float>(), st_, k, mode, err_, 0}, stream_);
-            return;
-        }
-    }
     if (s.engine == 1)
         launch_flat(s.tiling.dev, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
@@ -808,13 +755,6 @@ void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
 template <typename T, bool MAJOR>
 void Projector::launch_dual(const StepSide& s, int k, bool overlap) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    if constexpr (std::is_same<T, float>::value) {
-        if (s.engine == 2) {
-            launch_seg(s.seg, s.sl_log, s.seg_smem,
-                       DualOp<float, MAJOR, 256>{vecs<float>(), st_, M_.row_off, M_.n_eq, k, mode, err_, 0}, stream_);
-            return;
-        }
-    }
     if (s.engine == 1)
         launch_flat(s.tiling.dev, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
@@ -835,81 +775,8 @@ static int step_grid(const SideDev& d, int nt, int sms, bool async, bool half_re
     return tile_grid<OpT<T, true, 128>>(d, sms, async, half_red);
 }
 
-// Most clusters of a segmented-engine kernel resident at once (in CTAs), with `smem`
-// dynamic shared memory per CTA; sets the kernel's shared-memory attribute.
-template <class Op, int SL_LOG>
-static int seg_resident_ctas(size_t smem) {
-    auto kern = seg_spmv_kernel<Op, SL_LOG>;
-    PDFP_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(kSegQ * 64);
-    cfg.blockDim = dim3(kSegThreads);
-    cfg.dynamicSmemBytes = smem;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kSegQ;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    int ncl = 0;
-    PDFP_CK(cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg));
-    return ncl * kSegQ;
-}
-
-template <class OpMinor, class OpMajor>
-static int seg_prepare_kernels(int sl_log, size_t smem) {
-    if (sl_log == 14) {
-        seg_resident_ctas<OpMajor, 14>(smem);
-        return seg_resident_ctas<OpMinor, 14>(smem);
-    }
-    seg_resident_ctas<OpMajor, 13>(smem);
-    return seg_resident_ctas<OpMinor, 13>(smem);
-}
-
-// The segmented engine for an FP32 side of a one-instance handle: the layout is built
-// for as many CTAs as are resident at once with shared memory for up to kSegRowCap
-// rows and kSegWinCap windows per chunk; a side that needs more is left to the other
-// engines (grid 0).
-void Projector::prepare_seg_side(StepSide& s, bool primal) {
-    constexpr int kSegRowCap = 16384, kSegWinCap = 2048;
-    s.grid = 0;
-    s.sl_log = s.stage_bytes >= 65536 ? 14 : 13;
-    s.nt = kSegThreads;
-    s.gather_l2 = 3;
-    s.stages = 2;
-    s.half_red = false;
-    s.max_blocks = 0;
-    if (K_ != 1) return;
-    const size_t cap_smem = std::min<size_t>(seg_smem_bytes(s.sl_log, kSegRowCap, kSegWinCap),
-                                             static_cast<size_t>(max_smem_sm_) - 1024);
-    const int G = primal ? seg_prepare_kernels<PrimalOp<float, false, 256>, PrimalOp<float, true, 256>>(s.sl_log, cap_smem)
-                         : seg_prepare_kernels<DualOp<float, false, 256>, DualOp<float, true, 256>>(s.sl_log, cap_smem);
-    if (G < kSegQ) return;
-    SegHost h;
-    if (!build_seg_layout(primal ? M_.L.At : M_.L.A, G, kSegQ, s.sl_log, h).empty()) return;
-    s.seg_smem = seg_smem_bytes(h.sl_log, h.rmax, h.wmax);
-    if (s.seg_smem > cap_smem) return;
-    s.seg.G = h.G;
-    s.seg.S = h.S;
-    s.seg.sl_log = h.sl_log;
-    s.seg.rmax = h.rmax;
-    s.seg.wmax = h.wmax;
-    s.seg.ncols = h.ncols;
-    s.seg.row_start = ar_.upload(h.row_start);
-    s.seg.chunk_off = ar_.upload(h.chunk_off);
-    s.seg.key = ar_.upload(h.key);
-    s.seg.val = ar_.upload(h.val);
-    s.grid = h.G;
-}
-
 void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     const int e = f32 ? 4 : 8;
-    if (s.engine == 2) {
-        if (!f32) throw Error(E_INVALID, "internal: the segmented engine runs FP32 steps only");
-        prepare_seg_side(s, primal);
-        return;
-    }
     if (s.engine == 1) {
         const int cap = s.qpt * 4 * kFlatThreads;
         s.stage_bytes = flat_stage_bytes(e, cap);
@@ -994,10 +861,7 @@ void Projector::autotune(bool f32) {
         {0, 24 * 1024, 256, 0, 0, 2, 0, 1}, {0, 32 * 1024, 256, 1, 0, 2, 0, 1},
         // gather policy 2: per-thread async copies into the stage (FP32 steps)
         {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}, {0, 24 * 1024, 128, 2, 0, 3},
-        {0, 32 * 1024, 256, 2, 0, 4},
-        // the segmented engine: the gathered vector in cluster shared memory, 64 or 32 KB
-        // slices per CTA (FP32 steps of one-instance handles)
-        {2, 64 * 1024, kSegThreads, 3, 0, 2}, {2, 32 * 1024, kSegThreads, 3, 0, 2}};
+        {0, 32 * 1024, 256, 2, 0, 4}};
     constexpr int NC = sizeof(cands) / sizeof(cands[0]);
     cudaEvent_t e0, e1;
     PDFP_CK(cudaEventCreate(&e0));
@@ -1008,14 +872,7 @@ void Projector::autotune(bool f32) {
         std::vector<StepSide> sides(NC);
         std::vector<float> best_ms(NC, 1e30f);
         bool empty_side = false;
-        std::vector<bool> usable(NC, true);
-        const char* sg = std::getenv("PDFP_SEG");
-        const bool seg_ok = sg && sg[0] == '1';  // the segmented engine's candidates (PDFP_SEG=1)
         for (int i = 0; i < NC; ++i) {
-            if (cands[i].engine == 2 && (!f32 || K_ != 1 || !seg_ok)) {  // FP32 one-instance handles only
-                usable[i] = false;
-                continue;
-            }
             sides[i].engine = cands[i].engine;
             sides[i].stages = cands[i].stages;
             if (cands[i].engine == 1) sides[i].qpt = cands[i].qpt;
@@ -1025,10 +882,6 @@ void Projector::autotune(bool f32) {
             sides[i].max_blocks = cands[i].max_blocks;
             sides[i].half_red = cands[i].half_red != 0;
             prepare_side(sides[i], primal, f32);
-            if (cands[i].engine == 2) {
-                usable[i] = sides[i].grid > 0;  // the side does not fit the segmented layout
-                continue;
-            }
             if (sides[i].grid <= 0) empty_side = true;
         }
         StepSide& dst = primal ? (f32 ? p32_ : p64_) : (f32 ? d32_ : d64_);
@@ -1038,7 +891,6 @@ void Projector::autotune(bool f32) {
         }
         for (int sweep = 0; sweep < 2; ++sweep) {
             for (int i = 0; i < NC; ++i) {
-                if (!usable[i]) continue;
                 if (cands[i].l2 == 2 && !f32) continue;  // FP64 steps have no async policy
                 const StepSide& s = sides[i];
                 auto run = [&](int k) {
@@ -1064,7 +916,6 @@ void Projector::autotune(bool f32) {
         }
         int bi = 0;
         for (int i = 0; i < NC; ++i) {
-            if (!usable[i]) continue;
             tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, cands[i].stages,
                                           cands[i].max_blocks,
                                           sides[i].half_red ? cands[i].nt / 2 : cands[i].nt, best_ms[i]});

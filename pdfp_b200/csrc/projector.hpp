@@ -9,7 +9,6 @@
 #include "../../include/pdfp_b200.h"
 #include "device.hpp"
 #include "pdfp_ops.cuh"
-#include "seg_spmv.cuh"
 #include "state.hpp"
 
 namespace pdfp {
@@ -70,8 +69,7 @@ class Projector {
   private:
     // One side of the PDHG step: its tile geometry, block size and tiling.
     struct StepSide {
-        int engine = 0;  // 0: tile engine (tile_spmv.cuh), 1: flat engine (flat_spmv.cuh),
-                         // 2: segmented engine (seg_spmv.cuh; FP32, one instance)
+        int engine = 0;  // 0: tile engine (tile_spmv.cuh), 1: flat engine (flat_spmv.cuh)
         int qpt = 2;     // flat engine: quads (4 nonzeros) per thread and tile, 1 or 2
         int stages = 4;  // tile engine: shared-memory stages per block, 2..4
         int max_blocks = 0;  // tile engine: resident blocks per SM cap (0: as many as fit)
@@ -81,11 +79,8 @@ class Projector {
         int nt = 256;
         DeviceMatrix::Tiling tiling;
         int grid = 0;
-        int gather_l2 = 0;  // 3: the segmented engine's cluster shared memory
+        int gather_l2 = 0;
         float tuned_ms = 0.f;
-        SegDev seg{};       // engine 2: the side in the segmented layout
-        size_t seg_smem = 0;
-        int sl_log = 14;    // engine 2: log2 of each CTA's slice of a segment
     };
     struct TuneRow {
         int side, stage, nt, l2;  // nt = 0: the flat engine
@@ -102,7 +97,6 @@ class Projector {
     template <typename T, bool MAJOR>
     void launch_dual(const StepSide& s, int k, bool overlap = false);
     void prepare_side(StepSide& s, bool primal, bool f32);
-    void prepare_seg_side(StepSide& s, bool primal);
     void autotune(bool f32);
     void check_instance(int p) const;
     void check_unscaled(int p) const;

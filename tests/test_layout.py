@@ -92,59 +92,3 @@ def test_layout_many_short_rows(checker):
     A = sp.csr_matrix(sp.eye(20000) * 2.0)
     rc, tiles, _ = run(checker, [A], [np.ones(20000, bool)])
     assert rc == 0 and tiles > 5
-
-
-# ---- the segmented engine's layout (seg_spmv.cuh) ------------------------------------
-
-
-@pytest.fixture(scope="module")
-def seg_checker():
-    out = os.path.join(ROOT, "_build", "libseg_layout_check.so")
-    os.makedirs(os.path.dirname(out), exist_ok=True)
-    srcs = [os.path.join(HERE, "native", "seg_layout_check.cpp"),
-            os.path.join(ROOT, "pdfp_b200", "csrc", "layout.cpp")]
-    subprocess.run(["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-o", out] + srcs, check=True)
-    lib = C.CDLL(out)
-    lib.seg_layout_check.restype = C.c_int
-    return lib
-
-
-def seg_run(lib, A, G, q=8, sl_log=6):
-    A = sp.csr_matrix(A)
-    A.sort_indices()
-    m, n = A.shape
-    rp = np.ascontiguousarray(A.indptr, dtype=np.int32)
-    ci = np.ascontiguousarray(A.indices if A.nnz else np.zeros(1), dtype=np.int32)
-    v = np.ascontiguousarray(A.data if A.nnz else np.zeros(1), dtype=np.float64)
-    stats = (C.c_int64 * 2)()
-    rc = lib.seg_layout_check(m, n, rp.ctypes.data_as(C.POINTER(C.c_int32)),
-                              ci.ctypes.data_as(C.POINTER(C.c_int32)),
-                              v.ctypes.data_as(C.POINTER(C.c_double)), G, q, sl_log, stats)
-    return rc, stats[0], stats[1]
-
-
-@pytest.mark.parametrize("G,sl_log", [(8, 6), (16, 5), (64, 7), (8, 14)])
-def test_seg_layout_random(seg_checker, G, sl_log):
-    """Scattered columns, a few long rows (runs across many windows), empty rows."""
-    rng = np.random.default_rng(G + sl_log)
-    A = rand_csr(rng, 3000, 5000, 0.004, long_rows=5, long_len=900)
-    rc, S, cont = seg_run(seg_checker, A, G, sl_log=sl_log)
-    assert rc == 0
-    assert S == (5000 + (8 << sl_log) - 1) // (8 << sl_log)
-    if sl_log <= 7:
-        assert cont > 0  # continuation windows occur, so the fixup pass is exercised
-
-
-def test_seg_layout_zipf(seg_checker):
-    from pdfp_b200 import synthetic
-    milp, _ = synthetic.zipf_lp(seed=3, m=4000, n=20000, nnz=300_000)
-    for A in (milp.A, milp.A.T.tocsr()):
-        rc, _, cont = seg_run(seg_checker, A, 64, sl_log=8)
-        assert rc == 0 and cont > 0
-
-
-def test_seg_layout_rejects_what_does_not_fit(seg_checker):
-    A = sp.random(100, 300, density=0.05, random_state=np.random.default_rng(1), format="csr")
-    assert seg_run(seg_checker, A, 12)[0] == 1                    # not a multiple of the cluster
-    assert seg_run(seg_checker, A, 8, sl_log=15)[0] == 1          # 8 << 15 columns exceed 17 bits
-    assert seg_run(seg_checker, sp.csr_matrix((70000, 10)), 8)[0] == 1  # empty side
