@@ -439,27 +439,21 @@ def main():
                                                                 20_000_000)
         tun = mx["tuning"]
 
-        def kname(op, threads, policy):
-            if policy == 3:
-                return f"seg_spmv_kernel<{op}<float, false, 256>> (segmented engine)"
+        def kname(op, threads):
             return (f"flat_spmv_kernel<{op}<float, false, 256>>" if threads == 0
                     else f"tile_spmv_kernel<{op}<float, false, {threads}>>")
 
-        # DRAM bytes of one launch in the ncu captures of the default workload, per engine
-        # (profiles/): tile engine A' side 242.8 MB, A side 187.9 MB
-        captured = {("PrimalOp", 0): 242.8e6, ("DualOp", 0): 187.9e6}
         entries = []
-        for label, op, threads, policy, ms, byts in [
-                ("A'z + fused primal/y update", "PrimalOp", tun["a_t_threads"], tun["a_t_gather_l2"],
-                 mx["kp_ms"], bytes_primal32),
-                ("A x_bar + fused z update", "DualOp", tun["a_threads"], tun["a_gather_l2"],
-                 mx["kd_ms"], bytes_dual32)]:
+        for label, op, threads, ms, byts, traffic in [
+                ("A'z + fused primal/y update", "PrimalOp", tun["a_t_threads"], mx["kp_ms"],
+                 bytes_primal32, 242.8e6),
+                ("A x_bar + fused z update", "DualOp", tun["a_threads"], mx["kd_ms"],
+                 bytes_dual32, 187.9e6)]:
             achieved = byts / (ms * 1e-3) / 1e9
-            traffic = captured.get((op, 1 if policy == 3 else 0)) if threads else None
             entries.append({"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                             "unit": "GB/s", "frac": round(achieved / peak, 4),
                             "traffic": traffic if default else None,
-                            "kernel": f"{kname(op, threads, policy)} ({label})", "peak_kind": peak_kind,
+                            "kernel": f"{kname(op, threads)} ({label})", "peak_kind": peak_kind,
                             "bytes_per_launch": byts, "mean_launch_ms": round(ms, 5)})
         entries.sort(key=lambda e: -e["mean_launch_ms"])
         roof = dict(entries[0])
