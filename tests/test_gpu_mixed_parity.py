@@ -14,14 +14,10 @@ src/pdfp.jl:252-288) on the same targets:
   target with 5% of the integer targets flipped, warm-started;
 * config1: the 20k x 50k general-integer model (500k nonzeros).
 
-Each runs with the step engine the autotuner picks and, forced, with the
-segmented engine (PDFP_STEP_ENGINE=seg: the gathered vector in cluster shared
-memory), whose row sums add in a different order.
-
 Bars (the reference's own GPU-vs-CPU test is test/runtests.jl:81-88, the l1
 distance of src/pdfp.jl:210-217):
 
-* tight tolerance (1e-8 or 1e-7): the FP32 phase and the FP64 polish both run;
+* tight tolerance (1e-8; 1e-7 on config1): the FP32 phase and the FP64 polish both run;
   the l1 distance is within 1e-6 relative of the oracle's at the same
   tolerance; the KKT residuals re-evaluated in FP64 on the host meet it;
 * benchmark tolerance (gap and dual 1e-4, primal 1e-5): the solve stays in FP32;
@@ -109,16 +105,9 @@ def run_both(oracle, milp, targets, eps_opt, eps_feas, polish=None, key=None):
     return out
 
 
-@pytest.fixture(params=["auto", "seg"])
-def engine(request, monkeypatch):
-    """The step engine of the mixed handle: the autotuner's pick, or the segmented one."""
-    if request.param == "seg":
-        monkeypatch.setenv("PDFP_STEP_ENGINE", "seg")
-    return request.param
 
-
-@pytest.mark.parametrize("name,tol", [("zipf-4k", 1e-8), ("zipf-100k", 1e-7), ("config1", 1e-7)])
-def test_mixed_tight_matches_oracle(oracle, engine, name, tol):
+@pytest.mark.parametrize("name,tol", [("zipf-4k", 1e-8), ("zipf-100k", 1e-8), ("config1", 1e-7)])
+def test_mixed_tight_matches_oracle(oracle, name, tol):
     milp, targets = case(name)
     for r, (gp, gd, gg, gl1), ro, (op_, od, og, ol1), D in run_both(oracle, milp, targets, tol, tol,
                                                                     key=(name, tol)):
@@ -130,14 +119,14 @@ def test_mixed_tight_matches_oracle(oracle, engine, name, tol):
         # the device's FP64 distance is the host's
         assert r["objective_value"] == pytest.approx(gl1, rel=1e-9)
         rel = abs(gl1 - ol1) / ol1
-        print(f"\n[{name} {engine} tol {tol:g}] l1 gpu {gl1:.10g} oracle {ol1:.10g} rel {rel:.3e}; "
+        print(f"\n[{name} tol {tol:g}] l1 gpu {gl1:.10g} oracle {ol1:.10g} rel {rel:.3e}; "
               f"iterations {r['total_count']} ({r['fp64_iterations']} FP64) vs oracle "
               f"{ro['total_count']}")
         assert rel <= 1e-6
 
 
 @pytest.mark.parametrize("name", ["zipf-4k", "zipf-100k", "config1"])
-def test_mixed_at_bench_tolerance_stays_fp32(oracle, engine, name):
+def test_mixed_at_bench_tolerance_stays_fp32(oracle, name):
     eps_opt, eps_feas = BENCH_TOL
     milp, targets = case(name)
     for r, (gp, gd, gg, gl1), ro, (_, _, _, ol1), D in run_both(oracle, milp, targets, eps_opt,
@@ -146,7 +135,7 @@ def test_mixed_at_bench_tolerance_stays_fp32(oracle, engine, name):
         assert r["precision"] == 1  # PDFP_MIXED at termination
         assert gp <= eps_feas * 1.01 and gd <= eps_opt * 1.01 and gg <= eps_opt * 1.01
         diff = abs(gl1 - ol1)
-        print(f"\n[{name} {engine} bench tol] l1 gpu {gl1:.10g} oracle {ol1:.10g} rel {diff / ol1:.3e} "
+        print(f"\n[{name} bench tol] l1 gpu {gl1:.10g} oracle {ol1:.10g} rel {diff / ol1:.3e} "
               f"(bound {2 * eps_opt * D / ol1:.3e}); iterations {r['total_count']} vs oracle "
               f"{ro['total_count']}")
         assert diff <= 2.0 * eps_opt * D
@@ -182,24 +171,6 @@ def test_polish_off_runs_tight_tolerances_in_fp64(oracle):
     assert r["polished"] == 0 and r["fp64_iterations"] == r["total_count"]
     assert r["precision"] == 0
     assert abs(gl1 - ol1) <= 1e-6 * ol1
-
-
-def test_forced_segmented_engine_is_used(monkeypatch):
-    """PDFP_STEP_ENGINE=seg puts both FP32 sides of a one-instance handle on the segmented
-    engine (gather policy 3 in the tuning report); a batch handle keeps the tile engine."""
-    monkeypatch.setenv("PDFP_STEP_ENGINE", "seg")
-    milp, _ = synthetic.zipf_lp(seed=3, m=4000, n=20000, nnz=300_000)
-    from oracle import oracle as O
-    sc, is_eq, is_int, w = O.projector_inputs(milp)
-    g = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
-    assert tuple(g.tuning()[6:8]) == (3, 3)
-    b = gpu.PDFPBatch([(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w)] * 2,
-                      precision="mixed")
-    from pdfp_b200 import _lib as L
-    import ctypes as C
-    out = (C.c_int32 * 8)()
-    L.check(L.lib().pdfp_get_tuning(b._h, out))
-    assert 3 not in (out[6], out[7])
 
 
 def test_set_polish_rejects_bad_arguments():
