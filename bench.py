@@ -464,8 +464,10 @@ def main():
         roof["kernels_per_iteration_ms"] = round(mx["kp_ms"] + mx["kd_ms"], 5)
         roof["iteration_ms"] = round(ms_iter, 5)
         roof["kernel_share_of_iteration"] = round((mx["kp_ms"] + mx["kd_ms"]) / ms_iter, 4)
-        roof["sampling"] = ("CUDA events around both step kernels of 16 minor steps spread "
-                            "evenly over every evaluation window of the timed solves")
+        roof["sampling"] = ("per evaluation window of the timed solves: CUDA events around a run "
+                            "of its middle-half minor steps (no other event inside) give the mean "
+                            "step time, split between the two kernels in the proportion measured "
+                            "with events around each kernel of 8 single minor steps outside the run")
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,

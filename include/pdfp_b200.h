@@ -108,7 +108,7 @@ typedef struct {
     double device_ms;            /* device time of the solve: CUDA events on the handle's stream */
     double kernel_ms_primal;     /* timing mode: mean device time of the A'-side step kernel */
     double kernel_ms_dual;       /* timing mode: mean device time of the A-side step kernel */
-    int64_t kernel_samples;      /* timing mode: launches sampled per kernel */
+    int64_t kernel_samples;      /* timing mode: minor steps in the timed runs */
     int64_t fp64_iterations;     /* PDHG iterations of this solve run in FP64 (MIXED: the polish) */
 } pdfp_result;
 
@@ -208,9 +208,11 @@ PDFP_API int pdfp_shape(const pdfp_handle* h, int32_t instance, int32_t* k, int3
 PDFP_API int pdfp_destroy(pdfp_handle* h);
 
 /* Timing mode: when on, every evaluation window of later solves also records
- * CUDA events around both step launches of about sixteen minor steps spread
- * evenly over the window, and pdfp_result reports the mean duration of each
- * step kernel over them (benchmark support; off by default). */
+ * CUDA events around a run of its minor steps (the middle half of them, with no
+ * other event inside, so that they run as in any window) and around each kernel
+ * of up to eight single minor steps outside the run; pdfp_result reports the
+ * run's mean step time split between the two step kernels in the proportion of
+ * the single steps (benchmark support; off by default). */
 PDFP_API int pdfp_set_kernel_timing(pdfp_handle* h, int32_t on);
 
 /* Mixed precision (PDFP_MIXED handles): an instance starts each solve in FP32;

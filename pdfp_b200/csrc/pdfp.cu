@@ -1188,13 +1188,27 @@ void Projector::launch_medium_steps(int i0, int i1) {
                                static_cast<int32_t>(i1)));
 }
 
-// Timing mode samples the minor steps 2, 2 + every, 2 + 2 every, ... (at most
-// kTimedSteps of them) of a window of `freq` steps.
-int Projector::timed_step_every(int freq) { return std::max(1, (freq - 2) / kTimedSteps); }
-int Projector::timed_step_count(int freq) {
-    if (freq < 3) return 0;
-    const int every = timed_step_every(freq);
-    return std::min(kTimedSteps, (freq - 2 + every - 1) / every);
+// Timing mode's plan for a window of `freq` steps: the RUN, minor steps
+// [run_a, run_b) in the middle half of steps 2 .. freq-1, is bracketed by two events
+// and nothing else, so it times the average step as the other windows run it; up to
+// kSplitSteps single minor steps outside it (evenly spread, half before and half
+// after) get events around each kernel, and only the share of each kernel in them is
+// used, to split the run's step time between the two kernels.
+Projector::TimingPlan Projector::timing_plan(int freq) {
+    TimingPlan t{};
+    const int M = freq - 2;  // minor steps
+    if (M < 8) return t;
+    t.run_a = 2 + M / 4;
+    t.run_b = t.run_a + M / 2;
+    auto spread = [&](int a, int b) {  // up to kSplitSteps / 2 steps of [a, b)
+        const int len = b - a, want = kSplitSteps / 2;
+        const int every = std::max(1, len / want);
+        for (int i = a; i < b && t.n_split < kSplitSteps && (i - a) / every < want; i += every)
+            t.split[t.n_split++] = i;
+    };
+    spread(2, t.run_a);
+    spread(t.run_b + 1, freq);  // step run_b carries the run's closing event
+    return t;
 }
 
 void Projector::record_window(int freq, bool with32, bool with64) {
@@ -1228,12 +1242,11 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             launch_tile(ev_a_.dev, EvalRowOp<double, NT_EVAL>{v64_, ed_, st_, M_.row_off, M_.n_eq, which, mode64, err_}, g_.er, stream_);
         }
     };
-    // timing mode: events around both kernels of the sampled minor steps (about
-    // sixteen, spread evenly over steps 2 .. freq-1, so that the mean is the
-    // window's average step rather than the one after a restart)
-    const bool sample = timing_ && freq >= 3 && (with32 != with64);
-    const int sample_every = timed_step_every(freq);
-    int n_sampled = 0;
+    // timing mode (see timing_plan): a run of minor steps between two events, and
+    // single minor steps with events around each kernel for the split between them
+    const TimingPlan plan = timing_plan(freq);
+    const bool sample = timing_ && plan.run_b > plan.run_a && (with32 != with64);
+    int n_split = 0;
     for (int i = 1; i <= freq; ++i) {
         const bool major = (i == 1 || i == freq);
         if (tiny_ && !sample && i == 2 && freq > 2) {
@@ -1252,8 +1265,8 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             i = freq - 1;
             continue;
         }
-        if (sample && !major && (i - 2) % sample_every == 0 && n_sampled < kTimedSteps) {
-            cudaEvent_t* e = &tev_[3 * n_sampled];
+        if (sample && n_split < plan.n_split && i == plan.split[n_split]) {
+            cudaEvent_t* e = &tev_[2 + 3 * n_split];
             after_step = false;
             PDFP_CK(cudaEventRecordWithFlags(e[0], stream_, cudaEventRecordExternal));
             if (with32) prim32(i, major); else prim64(i, major);
@@ -1262,8 +1275,16 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             if (with32) dual32(i, major); else dual64(i, major);
             after_step = false;
             PDFP_CK(cudaEventRecordWithFlags(e[2], stream_, cudaEventRecordExternal));
-            ++n_sampled;
+            ++n_split;
             continue;
+        }
+        if (sample && i == plan.run_a) {
+            after_step = false;
+            PDFP_CK(cudaEventRecordWithFlags(tev_[0], stream_, cudaEventRecordExternal));
+        }
+        if (sample && i == plan.run_b) {
+            after_step = false;
+            PDFP_CK(cudaEventRecordWithFlags(tev_[1], stream_, cudaEventRecordExternal));
         }
         if (with32) { prim32(i, major); dual32(i, major); }
         if (with64) { prim64(i, major); dual64(i, major); }
@@ -1432,7 +1453,7 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     int32_t dev_err = 0;
     double kp_sum = 0.0, kd_sum = 0.0;
     int64_t k_samples = 0;
-    const int n_timed = timed_step_count(freq);
+    const TimingPlan plan = timing_plan(freq);
     for (;;) {
         bool running = false;
         for (int p = 0; p < K_; ++p) running = running || flags_h_[p].status == ST_RUNNING;
@@ -1448,15 +1469,20 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         polled = true;
         dev_err = flags_h_[K_].status;
         if (dev_err) throw Error(E_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
-        if (timing_ && freq >= 3 && (with32 != with64)) {
-            for (int t = 0; t < n_timed; ++t) {
+        if (timing_ && plan.run_b > plan.run_a && (with32 != with64)) {
+            float run = 0.f, sp = 0.f, sd = 0.f;
+            PDFP_CK(cudaEventElapsedTime(&run, tev_[0], tev_[1]));
+            for (int t = 0; t < plan.n_split; ++t) {
                 float a = 0.f, b = 0.f;
-                PDFP_CK(cudaEventElapsedTime(&a, tev_[3 * t], tev_[3 * t + 1]));
-                PDFP_CK(cudaEventElapsedTime(&b, tev_[3 * t + 1], tev_[3 * t + 2]));
-                kp_sum += a;
-                kd_sum += b;
-                ++k_samples;
+                PDFP_CK(cudaEventElapsedTime(&a, tev_[2 + 3 * t], tev_[3 + 3 * t]));
+                PDFP_CK(cudaEventElapsedTime(&b, tev_[3 + 3 * t], tev_[4 + 3 * t]));
+                sp += a;
+                sd += b;
             }
+            const double share = sp + sd > 0.f ? static_cast<double>(sp) / (sp + sd) : 0.5;
+            kp_sum += share * run;
+            kd_sum += (1.0 - share) * run;
+            k_samples += plan.run_b - plan.run_a;
         }
         // FP64 polish for instances whose FP32 progress stalled
         for (int p = 0; p < K_; ++p) {
@@ -1502,7 +1528,7 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         r.fp64_iterations = s.fp64_iters;
         r.precision = s.mode == MODE_FP32 ? PDFP_MIXED : PDFP_FP64;
         r.device_ms = solve_ms;
-        r.kernel_ms_primal = k_samples ? kp_sum / k_samples : 0.0;
+        r.kernel_ms_primal = k_samples ? kp_sum / k_samples : 0.0;  // the runs' step time, split
         r.kernel_ms_dual = k_samples ? kd_sum / k_samples : 0.0;
         r.kernel_samples = k_samples;
         vec_mode_[p] = s.mode;

@@ -105,8 +105,13 @@ class Projector {
     void load_cols(int p, T* dst, T* dst2, bool unscaled);
     void ensure_step_sizes(int32_t sv_max_iterations, double sv_tolerance);
     void record_window(int freq, bool with32, bool with64);
-    static int timed_step_every(int freq);
-    static int timed_step_count(int freq);
+    static constexpr int kSplitSteps = 8;  // timing mode: single steps timed per kernel per window
+    struct TimingPlan {
+        int run_a = 0, run_b = 0;  // the timed run of minor steps [run_a, run_b)
+        int split[kSplitSteps] = {};
+        int n_split = 0;
+    };
+    static TimingPlan timing_plan(int freq);
     template <typename T>
     void launch_tiny_steps(int i0, int i1);
     template <typename T>
@@ -161,8 +166,7 @@ class Projector {
     bool medium_ = false;  // a mid-sized handle: the minor steps in one cooperative launch
     int32_t *part_t_ = nullptr, *part_a_ = nullptr;  // each block's rows of A' and of A
     unsigned* gbar_ = nullptr;                          // the grid barrier's words
-    static constexpr int kTimedSteps = 16;                 // minor steps sampled per window (timing mode)
-    cudaEvent_t tev_[3 * kTimedSteps] = {};                // around each sampled step's two kernels
+    cudaEvent_t tev_[2 + 3 * kSplitSteps] = {};  // timing mode: the run's two, then 3 per split step
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
 };
 

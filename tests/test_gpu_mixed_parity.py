@@ -68,7 +68,7 @@ def case(name):
     return milp, [xt]
 
 
-_ORACLE_RUNS = {}  # the oracle's answers, shared by the engine variants of a case
+_ORACLE_RUNS = {}  # the oracle's answers by case and tolerance
 
 
 def run_both(oracle, milp, targets, eps_opt, eps_feas, polish=None, key=None):
