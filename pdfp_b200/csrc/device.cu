@@ -46,6 +46,47 @@ cudaMemPool_t current_pool() {
 }
 }  // namespace
 
+namespace {
+constexpr int kPinnedClasses = 32;
+constexpr size_t kPinnedKeep = 8;  // blocks kept per size class
+std::mutex g_pinned_mu;
+std::vector<void*> g_pinned_free[kPinnedClasses];
+int pinned_class(size_t bytes) {
+    int c = 0;
+    while ((size_t(256) << c) < bytes && c < kPinnedClasses - 1) ++c;
+    return c;
+}
+}  // namespace
+
+void* pinned_take(size_t bytes) {
+    const int c = pinned_class(bytes);
+    if ((size_t(256) << c) < bytes) throw Error(E_INVALID, "pinned block too large");
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        if (!g_pinned_free[c].empty()) {
+            void* p = g_pinned_free[c].back();
+            g_pinned_free[c].pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    PDFP_CK(cudaMallocHost(&p, size_t(256) << c));
+    return p;
+}
+
+void pinned_give(void* p, size_t bytes) {
+    if (!p) return;
+    const int c = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        if (g_pinned_free[c].size() < kPinnedKeep) {
+            g_pinned_free[c].push_back(p);
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
+
 void* arena_malloc(size_t bytes, bool* pooled) {
     void* p = nullptr;
     *pooled = false;

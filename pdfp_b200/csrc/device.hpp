@@ -42,23 +42,40 @@ void set_last_error(const std::string& msg);
 void* arena_malloc(size_t bytes, bool* pooled);
 void arena_free(const std::vector<void*>& ptrs, const std::vector<bool>& pooled);
 
-// Owns device allocations; every buffer is zero-filled and padded by 64 bytes
-// so that 16-byte-rounded bulk copies of any sub-range stay inside it.
+// Page-locked host blocks for the handles' small poll buffers, kept for reuse by size
+// class (powers of two from 256 bytes): pinning host memory costs tens of
+// microseconds and unpinning it waits for the device, which a pump run's short-lived
+// handles would otherwise pay each time.  The blocks are not zeroed.
+void* pinned_take(size_t bytes);
+void pinned_give(void* p, size_t bytes);
+
+// Owns device allocations; every buffer is zero-filled, starts 256-byte aligned and
+// is padded by 64 bytes so that 16-byte-rounded bulk copies of any sub-range stay
+// inside it.  Buffers up to kSmallBytes are carved out of kSlabBytes slabs, each
+// zero-filled once: a small handle's dozens of buffers then cost a couple of
+// allocations and host waits instead of one each.
 class DeviceArena {
   public:
+    static constexpr size_t kSlabBytes = size_t(1) << 20;
+    static constexpr size_t kSmallBytes = size_t(128) << 10;
     DeviceArena() = default;
     DeviceArena(const DeviceArena&) = delete;
     DeviceArena& operator=(const DeviceArena&) = delete;
     ~DeviceArena() { release(); }
     template <class T>
     T* alloc(size_t n) {
-        size_t bytes = ((n * sizeof(T) + 63) & ~size_t(63)) + 64;
-        bool pooled = false;
-        void* p = arena_malloc(bytes, &pooled);
-        ptrs_.push_back(p);
-        pooled_.push_back(pooled);
+        const size_t bytes = ((n * sizeof(T) + 63) & ~size_t(63)) + 64;
         bytes_ += bytes;
-        return static_cast<T*>(p);
+        if (bytes <= kSmallBytes) {
+            const size_t off = (slab_used_ + 255) & ~size_t(255);
+            if (!slab_ || off + bytes > kSlabBytes) {
+                slab_ = static_cast<unsigned char*>(take(kSlabBytes));
+                slab_used_ = 0;
+                return carve<T>(0, bytes);
+            }
+            return carve<T>(off, bytes);
+        }
+        return static_cast<T*>(take(bytes));
     }
     template <class T>
     T* upload(const std::vector<T>& h) {
@@ -71,10 +88,26 @@ class DeviceArena {
         ptrs_.clear();
         pooled_.clear();
         bytes_ = 0;
+        slab_ = nullptr;
+        slab_used_ = 0;
     }
     size_t bytes() const { return bytes_; }
 
   private:
+    void* take(size_t bytes) {
+        bool pooled = false;
+        void* p = arena_malloc(bytes, &pooled);
+        ptrs_.push_back(p);
+        pooled_.push_back(pooled);
+        return p;
+    }
+    template <class T>
+    T* carve(size_t off, size_t bytes) {
+        slab_used_ = off + bytes;
+        return reinterpret_cast<T*>(slab_ + off);
+    }
+    unsigned char* slab_ = nullptr;  // the slab small buffers are carved from
+    size_t slab_used_ = 0;
     std::vector<void*> ptrs_;
     std::vector<bool> pooled_;
     size_t bytes_ = 0;

@@ -567,10 +567,10 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     has_col_scale_.assign(K_, false);
     sp_ = ar_.alloc<SolveParams>(K_);
     stage_ = ar_.alloc<double>(std::max<int64_t>(std::max(M_.max_m, M_.max_n), 1));
-    PDFP_CK(cudaMallocHost(&flags_h_, sizeof(InstFlags) * (K_ + 1)));
-    PDFP_CK(cudaMallocHost(&st_h_, sizeof(InstState) * K_));
+    flags_h_ = static_cast<InstFlags*>(pinned_take(sizeof(InstFlags) * (K_ + 1)));
+    st_h_ = static_cast<InstState*>(pinned_take(sizeof(InstState) * K_));
     host_total_.assign(K_, 0);
-    PDFP_CK(cudaMallocHost(&nan_seen_h_, sizeof(int32_t)));
+    nan_seen_h_ = static_cast<int32_t*>(pinned_take(sizeof(int32_t)));
     vec_mode_.assign(K_, precision_ == PDFP_MIXED ? MODE_FP32 : MODE_FP64);
 
     // per-instance data vectors (permuted into packed order)
@@ -651,7 +651,6 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     ed_.val_a = M_.v64_a;
     ed_.part_col = part_col_;
     ed_.part_row = part_row_;
-    for (auto& e : tev_) PDFP_CK(cudaEventCreate(&e));
     for (auto& e : sev_) PDFP_CK(cudaEventCreate(&e));
     PDFP_CK(cudaDeviceSynchronize());
     // The autotuner pays for itself only where a step kernel takes longer than its
@@ -990,9 +989,9 @@ Projector::~Projector() {
     for (auto& e : sev_) if (e) cudaEventDestroy(e);
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     graphs_.clear();
-    if (flags_h_) cudaFreeHost(flags_h_);
-    if (st_h_) cudaFreeHost(st_h_);
-    if (nan_seen_h_) cudaFreeHost(nan_seen_h_);
+    pinned_give(flags_h_, sizeof(InstFlags) * (K_ + 1));
+    pinned_give(st_h_, sizeof(InstState) * K_);
+    pinned_give(nan_seen_h_, sizeof(int32_t));
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1002,6 +1001,13 @@ void Projector::set_polish(int32_t stall_evaluations, double fp32_floor) {
         throw Error(E_INVALID, "fp32_floor must lie in (0, 1)");
     stall_limit_ = stall_evaluations;
     fp32_floor_ = fp32_floor;
+}
+
+// The timing mode's events are made the first time it is switched on.
+void Projector::set_kernel_timing(bool on) {
+    if (on && !tev_[0])
+        for (auto& e : tev_) PDFP_CK(cudaEventCreate(&e));
+    timing_ = on;
 }
 
 void Projector::check_instance(int p) const {

@@ -64,7 +64,7 @@ class Projector {
     // stage bytes, gatherer threads, gather policy, stages, blocks per SM cap,
     // reducer threads}; returns the count.
     int tuning_table(float* ms, int32_t* cfg, int cap) const;
-    void set_kernel_timing(bool on) { timing_ = on; }
+    void set_kernel_timing(bool on);
 
   private:
     // One side of the PDHG step: its tile geometry, block size and tiling.
