@@ -344,21 +344,26 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
         _log("rounder     %s schedule, violation-guided rounding %s (first rounding violates by %.4g)\n" % (
             rounder.schedule, "off" if rounder.direction is None else "on", total_violation))
 
-    # The projector, built once (:293-307).
-    is_eq = milp.is_eq
-    is_int = milp.is_int
-    con_lb = np.where(is_eq, milp.b, -np.inf)
-    sp_ = solvers.scale_problem(milp.A, np.zeros(n), milp.l.copy(), milp.u.copy(), con_lb,
-                                milp.b.copy(), bound_objective_rescaling=False)
-    D_c = sp_.D_c
-    weights = np.ones(n)
-    weights[int_idx] = D_c[int_idx]
-    projector = solvers.PDFPState(sp_.A, sp_.con_ub, is_eq, is_int, sp_.var_lb, sp_.var_ub,
-                                  weights, precision=precision)
-    if mixed:
-        projector.original_primal_residual(sp_.D_r)
-    scaling = _ColumnScaling(projector, D_c)
-    scaling.set_x(x)
+    # The projector (:293-307), built once -- at the first projection, so that a run
+    # whose first rounding is already feasible does not pay for it.
+    def build_projector():
+        is_eq = milp.is_eq
+        is_int = milp.is_int
+        con_lb = np.where(is_eq, milp.b, -np.inf)
+        sp_ = solvers.scale_problem(milp.A, np.zeros(n), milp.l.copy(), milp.u.copy(), con_lb,
+                                    milp.b.copy(), bound_objective_rescaling=False)
+        D_c = sp_.D_c
+        weights = np.ones(n)
+        weights[int_idx] = D_c[int_idx]
+        proj = solvers.PDFPState(sp_.A, sp_.con_ub, is_eq, is_int, sp_.var_lb, sp_.var_ub,
+                                 weights, precision=precision)
+        if mixed:
+            proj.original_primal_residual(sp_.D_r)
+        sc = _ColumnScaling(proj, D_c)
+        sc.set_x(x)
+        return proj, sc
+
+    projector = scaling = None
     primal_weight = math.sqrt(1.0 + (len(int_idx) / m if m > 0 else 0.0))
     gap = gap_start
     tightening_budget = gap_start
@@ -383,6 +388,8 @@ def feasibility_pump(milp: MILP, *, time_limit: float = 1800.0, seed: int = 1,
         since_restart += 1
 
         # Project x~ onto the LP relaxation (:329-363).
+        if projector is None:
+            projector, scaling = build_projector()
         t = time.time()
         scaling.set_target(xt)
         gap_used = gap
@@ -559,19 +566,25 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
     trajs = [_Trajectory(milp, s, x, dual_slack, push_threshold, violation_threshold,
                          propagation_budget, swap_iteration, batch_policy, flip_parameter, mixed)
              for s in seeds]
-    is_eq, is_int = milp.is_eq, milp.is_int
-    con_lb = np.where(is_eq, milp.b, -np.inf)
-    sp_ = solvers.scale_problem(milp.A, np.zeros(n), milp.l.copy(), milp.u.copy(), con_lb,
-                                milp.b.copy(), bound_objective_rescaling=False)
-    D_c = sp_.D_c
-    weights = np.ones(n)
-    weights[int_idx] = D_c[int_idx]
-    ru = (1.0 / sp_.D_r) if mixed else None
-    prob = (sp_.A, sp_.con_ub, is_eq, is_int, sp_.var_lb, sp_.var_ub, weights, ru)
-    batch = solvers.PDFPBatch([prob] * K, precision=precision)
-    scalings = [_ColumnScaling(batch, D_c, p) for p in range(K)]
-    for p in range(K):
-        scalings[p].set_x(x)
+    # the projector batch, built at the first projection (a run whose first roundings
+    # are already feasible does not pay for it)
+    def build_batch():
+        is_eq, is_int = milp.is_eq, milp.is_int
+        con_lb = np.where(is_eq, milp.b, -np.inf)
+        sp_ = solvers.scale_problem(milp.A, np.zeros(n), milp.l.copy(), milp.u.copy(), con_lb,
+                                    milp.b.copy(), bound_objective_rescaling=False)
+        D_c = sp_.D_c
+        weights = np.ones(n)
+        weights[int_idx] = D_c[int_idx]
+        ru = (1.0 / sp_.D_r) if mixed else None
+        prob = (sp_.A, sp_.con_ub, is_eq, is_int, sp_.var_lb, sp_.var_ub, weights, ru)
+        b = solvers.PDFPBatch([prob] * K, precision=precision)
+        scs = [_ColumnScaling(b, D_c, p) for p in range(K)]
+        for p in range(K):
+            scs[p].set_x(x)
+        return b, scs
+
+    batch = scalings = None
     primal_weight = math.sqrt(1.0 + (len(int_idx) / m if m > 0 else 0.0))
     gaps = [gap_start] * K
     budgets = [gap_start] * K
@@ -594,6 +607,8 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
                 break
         if winner is not None:
             continue
+        if batch is None:
+            batch, scalings = build_batch()
         for p, tr in enumerate(trajs):
             tr.iterations += 1
             tr.since_restart += 1
