@@ -272,23 +272,133 @@ struct WarmStartCopy {  // initial = current (src/pdfp.jl:105-107)
 // max_windows windows have run.  The passes are tiny_pass (the one-block steps) and
 // tiny_eval_pass; the controller is the window's own (Controller::finalize), on the
 // block-summed terms.
+//
+// STAGED: the member's iterates, data and both sides of its matrix are copied into
+// the block's shared memory for the launch (and the iterates back at its end), so that
+// no pass waits on a global-memory round trip for what the previous pass wrote; the
+// arithmetic is the same, so the results are bit-identical to the unstaged kernel.
 constexpr int kTinyWindowsPerLaunch = 64;
 
+// Shared-memory bytes of a member's staged copy (tiny_solve_kernel<T, true>).
 template <typename T>
+__host__ __device__ inline size_t tiny_stage_bytes(int64_t nc, int64_t nr, int64_t nzt, int64_t nza,
+                                                   bool unscale) {
+    auto r16 = [](int64_t b) { return static_cast<size_t>((b + 15) & ~int64_t(15)); };
+    size_t b = 13 * r16(sizeof(T) * nc) + 5 * r16(sizeof(T) * nr);  // iterates and data
+    b += r16(4 * (nc + 1)) + r16(4 * (nr + 1)) + r16(4 * nzt) + r16(4 * nza);  // pointers, indices
+    b += r16(sizeof(T) * nzt) + r16(sizeof(T) * nza);                       // values
+    if (sizeof(T) == 4) b += 2 * r16(8 * nc) + r16(8 * nr) + r16(8 * nzt) + r16(8 * nza);  // FP64 copies
+    if (unscale) b += r16(8 * nr);
+    return b;
+}
+
+template <typename T, bool STAGED>
 __global__ void __launch_bounds__(kTinyThreads)
-    tiny_solve_kernel(IterVecs<T> v, EvalData ed, InstState* st, InstFlags* fl,
-                      const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
-                      const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
+    tiny_solve_kernel(IterVecs<T> gv, EvalData ged, InstState* st, InstFlags* fl,
+                      const int32_t* __restrict__ g_rp_t, const int32_t* __restrict__ g_ci_t,
+                      const int32_t* __restrict__ g_rp_a, const int32_t* __restrict__ g_ci_a,
                       const int32_t* __restrict__ col_off, const int32_t* __restrict__ row_off,
                       const int32_t* __restrict__ n_eq, int32_t* err, int32_t max_windows,
-                      int32_t polish) {
+                      int32_t polish, int32_t rowsum_len) {
     constexpr int NT = kTinyThreads;
     constexpr int32_t mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    extern __shared__ __align__(16) double tiny_rowsum[];  // 2 * max(rows, columns) of a member
+    extern __shared__ __align__(16) double tiny_rowsum[];  // rowsum_len doubles, then the staged copy
     __shared__ double red[8 * (NT / 32)];
     __shared__ int32_t go;
     const int p = blockIdx.x;
     const int32_t c0 = col_off[p], c1 = col_off[p + 1], r0 = row_off[p], r1 = row_off[p + 1];
+    IterVecs<T> v = gv;
+    EvalData ed = ged;
+    const int32_t *rp_t = g_rp_t, *ci_t = g_ci_t, *rp_a = g_rp_a, *ci_a = g_ci_a;
+    const int32_t nc = c1 - c0, nr = r1 - r0;
+    T* const stv[9] = {gv.cx, gv.ix, gv.px, gv.rx, gv.cy, gv.iy, gv.py, gv.ry, gv.ds};  // n-side iterates
+    T* const stz[4] = {gv.cz, gv.iz, gv.pz, gv.rz};                                      // m-side iterates
+    T* loc_v[9] = {};
+    T* loc_z[4] = {};
+    if constexpr (STAGED) {
+        // carve the copy out of the shared memory after the row sums; every region
+        // starts 16-byte aligned; pointers are rebased so that the packed indices the
+        // Ops use land in the copy
+        unsigned char* cur = reinterpret_cast<unsigned char*>(tiny_rowsum + rowsum_len);
+        auto carve = [&](size_t bytes) {
+            unsigned char* q = cur;
+            cur += (bytes + 15) & ~size_t(15);
+            return q;
+        };
+        const int32_t k0t = g_rp_t[c0], k1t = g_rp_t[c1], k0a = g_rp_a[r0], k1a = g_rp_a[r1];
+        auto stage_n = [&](const T* src) {
+            T* d = reinterpret_cast<T*>(carve(sizeof(T) * nc));
+            for (int32_t i = threadIdx.x; i < nc; i += NT) d[i] = src[c0 + i];
+            return d;
+        };
+        auto stage_m = [&](const T* src) {
+            T* d = reinterpret_cast<T*>(carve(sizeof(T) * nr));
+            for (int32_t i = threadIdx.x; i < nr; i += NT) d[i] = src[r0 + i];
+            return d;
+        };
+        for (int k = 0; k < 9; ++k) loc_v[k] = stage_n(stv[k]);
+        for (int k = 0; k < 4; ++k) loc_z[k] = stage_m(stz[k]);
+        T* lb = stage_n(gv.lb);
+        T* ub = stage_n(gv.ub);
+        T* xt = stage_n(gv.xt);
+        T* w = stage_n(gv.w);
+        T* b = stage_m(gv.b);
+        int32_t* rpt = reinterpret_cast<int32_t*>(carve(4 * (nc + 1)));
+        int32_t* rpa = reinterpret_cast<int32_t*>(carve(4 * (nr + 1)));
+        int32_t* cit = reinterpret_cast<int32_t*>(carve(4 * (k1t - k0t)));
+        int32_t* cia = reinterpret_cast<int32_t*>(carve(4 * (k1a - k0a)));
+        T* vt = reinterpret_cast<T*>(carve(sizeof(T) * (k1t - k0t)));
+        T* va = reinterpret_cast<T*>(carve(sizeof(T) * (k1a - k0a)));
+        for (int32_t i = threadIdx.x; i <= nc; i += NT) rpt[i] = g_rp_t[c0 + i];
+        for (int32_t i = threadIdx.x; i <= nr; i += NT) rpa[i] = g_rp_a[r0 + i];
+        for (int32_t k = threadIdx.x; k < k1t - k0t; k += NT) {
+            cit[k] = g_ci_t[k0t + k];
+            vt[k] = gv.val_t[k0t + k];
+        }
+        for (int32_t k = threadIdx.x; k < k1a - k0a; k += NT) {
+            cia[k] = g_ci_a[k0a + k];
+            va[k] = gv.val_a[k0a + k];
+        }
+        T** vp[9] = {&v.cx, &v.ix, &v.px, &v.rx, &v.cy, &v.iy, &v.py, &v.ry, &v.ds};
+        for (int k = 0; k < 9; ++k) *vp[k] = loc_v[k] - c0;
+        T** zp[4] = {&v.cz, &v.iz, &v.pz, &v.rz};
+        for (int k = 0; k < 4; ++k) *zp[k] = loc_z[k] - r0;
+        v.lb = lb - c0;
+        v.ub = ub - c0;
+        v.xt = xt - c0;
+        v.w = w - c0;
+        v.b = b - r0;
+        v.val_t = vt - k0t;
+        v.val_a = va - k0a;
+        rp_t = rpt - c0;
+        rp_a = rpa - r0;
+        ci_t = cit - k0t;
+        ci_a = cia - k0a;
+        if constexpr (std::is_same<T, double>::value) {  // the FP64 data are these very arrays
+            ed.xt = v.xt;
+            ed.w = v.w;
+            ed.b = v.b;
+            ed.val_t = v.val_t;
+            ed.val_a = v.val_a;
+        } else {
+            auto stage64 = [&](const double* src, int64_t off, int64_t len) {
+                double* d = reinterpret_cast<double*>(carve(8 * len));
+                for (int64_t i = threadIdx.x; i < len; i += NT) d[i] = src[off + i];
+                return d - off;
+            };
+            ed.xt = stage64(ged.xt, c0, nc);
+            ed.w = stage64(ged.w, c0, nc);
+            ed.b = stage64(ged.b, r0, nr);
+            ed.val_t = stage64(ged.val_t, k0t, k1t - k0t);
+            ed.val_a = stage64(ged.val_a, k0a, k1a - k0a);
+        }
+        if (ged.row_unscale) {
+            double* d = reinterpret_cast<double*>(carve(8 * nr));
+            for (int32_t i = threadIdx.x; i < nr; i += NT) d[i] = ged.row_unscale[r0 + i];
+            ed.row_unscale = d - r0;
+        }
+        __syncthreads();
+    }
     // the evaluation terms of one phase, block-summed, then the controller (thread 0)
     auto evaluate = [&](int32_t which, int32_t phase) {
         double ac[8], ar[4];
@@ -333,6 +443,13 @@ __global__ void __launch_bounds__(kTinyThreads)
         if (threadIdx.x == 0) go = st[p].status == ST_RUNNING && !fl[p].polish_request;
         __syncthreads();
         if (!go) break;
+    }
+    if constexpr (STAGED) {  // the iterates back to global memory
+        __syncthreads();
+        for (int k = 0; k < 9; ++k)
+            for (int32_t i = threadIdx.x; i < nc; i += NT) stv[k][c0 + i] = loc_v[k][i];
+        for (int k = 0; k < 4; ++k)
+            for (int32_t i = threadIdx.x; i < nr; i += NT) stz[k][r0 + i] = loc_z[k][i];
     }
 }
 
@@ -1323,25 +1440,53 @@ void Projector::prepare_window() {
 // handle replays one window's captured graph.
 void Projector::run_window(int freq, bool with32, bool with64) {
     if (tiny_ && !timing_) {
-        const size_t smem = sizeof(double) * 2 * static_cast<size_t>(std::max(M_.max_m, M_.max_n));
+        const int32_t rowsum_len = 2 * std::max(M_.max_m, M_.max_n);
         if (!window_ready_) {
-            if (smem > 48 * 1024) {
-                PDFP_CK(cudaFuncSetAttribute(tiny_solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem)));
-                PDFP_CK(cudaFuncSetAttribute(tiny_solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem)));
+            // the staged form when every member's copy fits next to the row sums
+            // (PDFP_TINY_STAGE=0 switches it off)
+            const char* ts = std::getenv("PDFP_TINY_STAGE");
+            const bool want = !(ts && ts[0] == '0');
+            const HostLayout& L = M_.L;
+            size_t s32 = 0, s64 = 0;
+            for (int p = 0; p < K_; ++p) {
+                const int64_t nc = L.col_off[p + 1] - L.col_off[p], nr = L.row_off[p + 1] - L.row_off[p];
+                const int64_t nzt = L.At.rp[L.col_off[p + 1]] - L.At.rp[L.col_off[p]];
+                const int64_t nza = L.A.rp[L.row_off[p + 1]] - L.A.rp[L.row_off[p]];
+                const bool un = row_unscale_ != nullptr;
+                s32 = std::max(s32, tiny_stage_bytes<float>(nc, nr, nzt, nza, un));
+                s64 = std::max(s64, tiny_stage_bytes<double>(nc, nr, nzt, nza, un));
             }
+            const size_t base = sizeof(double) * static_cast<size_t>(rowsum_len);
+            const size_t cap = static_cast<size_t>(max_smem_sm_) - 8 * 1024;
+            tiny_smem32_ = want && base + s32 <= cap ? base + s32 : base;
+            tiny_smem64_ = want && base + s64 <= cap ? base + s64 : base;
+            tiny_staged32_ = tiny_smem32_ > base;
+            tiny_staged64_ = tiny_smem64_ > base;
+            auto attr = [&](auto kern, size_t bytes) {
+                if (bytes > 48 * 1024)
+                    PDFP_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(bytes)));
+            };
+            if (tiny_staged32_) attr(tiny_solve_kernel<float, true>, tiny_smem32_);
+            else attr(tiny_solve_kernel<float, false>, tiny_smem32_);
+            if (tiny_staged64_) attr(tiny_solve_kernel<double, true>, tiny_smem64_);
+            else attr(tiny_solve_kernel<double, false>, tiny_smem64_);
             window_ready_ = true;
         }
         (void)freq;  // each member's own evaluation frequency (its state) drives the kernel
-        if (with32)
-            tiny_solve_kernel<float><<<K_, kTinyThreads, smem, stream_>>>(
-                v32_, ed_, st_, flags_, M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, M_.n_eq,
-                err_, kTinyWindowsPerLaunch, polish_enabled_);
-        if (with64)
-            tiny_solve_kernel<double><<<K_, kTinyThreads, smem, stream_>>>(
-                v64_, ed_, st_, flags_, M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, M_.col_off, M_.row_off, M_.n_eq,
-                err_, kTinyWindowsPerLaunch, polish_enabled_);
+        auto launch = [&](auto kern, auto& vecs, size_t bytes) {
+            kern<<<K_, kTinyThreads, bytes, stream_>>>(vecs, ed_, st_, flags_, M_.rp_t, M_.ci_t, M_.rp_a,
+                                                       M_.ci_a, M_.col_off, M_.row_off, M_.n_eq, err_,
+                                                       kTinyWindowsPerLaunch, polish_enabled_, rowsum_len);
+        };
+        if (with32) {
+            if (tiny_staged32_) launch(tiny_solve_kernel<float, true>, v32_, tiny_smem32_);
+            else launch(tiny_solve_kernel<float, false>, v32_, tiny_smem32_);
+        }
+        if (with64) {
+            if (tiny_staged64_) launch(tiny_solve_kernel<double, true>, v64_, tiny_smem64_);
+            else launch(tiny_solve_kernel<double, false>, v64_, tiny_smem64_);
+        }
         PDFP_CK(cudaGetLastError());
         return;
     }

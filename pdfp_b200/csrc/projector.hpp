@@ -119,7 +119,9 @@ class Projector {
     cudaGraphExec_t window_graph(int freq, bool with32, bool with64);
     void prepare_window();
     void run_window(int freq, bool with32, bool with64);
-    bool window_ready_ = false;  // prepare_window ran (direct windows)
+    bool window_ready_ = false;  // the whole-window kernels' launch shape is set
+    size_t tiny_smem32_ = 0, tiny_smem64_ = 0;      // their dynamic shared memory
+    bool tiny_staged32_ = false, tiny_staged64_ = false;  // members copied into shared memory
 
     int precision_;
     int K_ = 0;

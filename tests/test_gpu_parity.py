@@ -374,3 +374,35 @@ def test_uneven_batch_members_follow_the_oracle(oracle):
         status = twin.solve(prm, 1.0)
         assert st[p] == status and b.results[p]["total_count"] == twin.total_count, p
         assert np.abs(b.get(p, "pdhg_x") - twin.pdhg_x).max() <= 1e-10, p
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_whole_window_kernel_staged_equals_unstaged(oracle, monkeypatch, precision):
+    """Small members run whole windows in one launch, with their vectors and matrix
+    copied into shared memory for the launch or read in place (PDFP_TINY_STAGE=0): the
+    same arithmetic, so bit-identical iterates and the same iteration counts."""
+    milps = [synthetic.covering_p0201_like(s) for s in (1, 2)] + [synthetic.markshare_like(3)]
+    targets = [np.round(np.random.default_rng(s).random(len(m.c))) for s, m in zip((5, 6, 7), milps)]
+    out = {}
+    for stage in ("1", "0"):
+        monkeypatch.setenv("PDFP_TINY_STAGE", stage)
+        probs, dcs = [], []
+        for m in milps:
+            sc, is_eq, is_int, w = proj_inputs(oracle, m)
+            probs.append((sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w))
+            dcs.append(sc.D_c)
+        b = gpu.PDFPBatch(probs, precision=precision)
+        for p, xt in enumerate(targets):
+            b.set_target(p, xt / dcs[p])
+        b.solve(SolverParameters(eps_optimal_relative=1e-6, eps_feasible_relative=1e-6,
+                                 iteration_limit=100_000), 1.0)
+        single = gpu.PDFPState(*probs[0], precision=precision)
+        single.set_target(targets[0] / dcs[0])
+        single.solve(SolverParameters(eps_optimal_relative=1e-6, eps_feasible_relative=1e-6), 1.0)
+        out[stage] = ([r["total_count"] for r in b.results], [b.get(p, "pdhg_x") for p in range(3)],
+                      single.total_count, single.pdhg_x)
+    (c1, x1, s1, y1), (c0, x0, s0, y0) = out["1"], out["0"]
+    assert c1 == c0 and s1 == s0
+    for a, bb in zip(x1, x0):
+        assert np.array_equal(a, bb)
+    assert np.array_equal(y1, y0)
