@@ -244,20 +244,94 @@ struct LpRestartCopy {
 // windows of pdlp_solve! (src/pdlp.jl:332-370) -- step 1, the evaluation after a
 // restart, steps 2 .. freq-1, step freq, the full evaluation, the cuPDLPx ray passes,
 // the controller and the restart copy -- until the LP stops, asks for the FP64 polish,
-// or max_windows windows have run.
+// or max_windows windows have run.  STAGED: the LP's iterates, data, ray work vectors
+// and matrix are copied into the block's shared memory for the launch (the iterates
+// back at its end): the same arithmetic, bit-identical results.
 constexpr int kLpTinyWindowsPerLaunch = 64;
 
+// Shared-memory bytes of an LP's staged copy (lp_tiny_solve_kernel<T, true>).
 template <typename T>
+inline size_t lp_tiny_stage_bytes(int64_t n, int64_t m, int64_t nnz, bool unscale) {
+    auto r16 = [](int64_t b) { return static_cast<size_t>((b + 15) & ~int64_t(15)); };
+    size_t b = 8 * r16(sizeof(T) * n) + 6 * r16(sizeof(T) * m);          // iterates and data
+    b += r16(4 * (n + 1)) + r16(4 * (m + 1)) + 2 * r16(4 * nnz) + 2 * r16(sizeof(T) * nnz);
+    b += r16(8 * n) + r16(8 * m);                                         // ray work vectors
+    if (sizeof(T) == 4) b += 3 * r16(8 * n) + 2 * r16(8 * m) + 2 * r16(8 * nnz);  // FP64 copies
+    if (unscale) b += r16(8 * n) + r16(8 * m);
+    return b;
+}
+
+template <typename T, bool STAGED>
 __global__ void __launch_bounds__(kTinyThreads)
-    lp_tiny_solve_kernel(LpVecs<T> v, LpData d, InstState* st, InstFlags* fl,
-                         const int32_t* __restrict__ rp_t, const int32_t* __restrict__ ci_t,
-                         const int32_t* __restrict__ rp_a, const int32_t* __restrict__ ci_a,
-                         int32_t n, int32_t m, int32_t* err, int32_t cupdlpx, int32_t max_windows) {
+    lp_tiny_solve_kernel(LpVecs<T> gv, LpData gd, InstState* st, InstFlags* fl,
+                         const int32_t* __restrict__ g_rp_t, const int32_t* __restrict__ g_ci_t,
+                         const int32_t* __restrict__ g_rp_a, const int32_t* __restrict__ g_ci_a,
+                         int32_t n, int32_t m, int32_t* err, int32_t cupdlpx, int32_t max_windows,
+                         int32_t rowsum_len) {
     constexpr int NT = kTinyThreads;
     constexpr int32_t mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
-    extern __shared__ __align__(16) double lp_rowsum[];  // 2 * max(n, m)
+    extern __shared__ __align__(16) double lp_rowsum[];  // rowsum_len doubles, then the staged copy
     __shared__ double red[8 * (NT / 32)];
     __shared__ int32_t go;
+    LpVecs<T> v = gv;
+    LpData d = gd;
+    const int32_t *rp_t = g_rp_t, *ci_t = g_ci_t, *rp_a = g_rp_a, *ci_a = g_ci_a;
+    T* const gx[5] = {gv.cx, gv.ix, gv.px, gv.rx, gv.ds};  // n-side iterates
+    T* const gy[4] = {gv.cy, gv.iy, gv.py, gv.ry};         // m-side iterates
+    T* sx[5] = {};
+    T* sy[4] = {};
+    if constexpr (STAGED) {
+        unsigned char* cur = reinterpret_cast<unsigned char*>(lp_rowsum + rowsum_len);
+        auto carve = [&](size_t bytes) {
+            unsigned char* q = cur;
+            cur += (bytes + 15) & ~size_t(15);
+            return q;
+        };
+        auto stage = [&](const auto* src, int64_t len) {
+            using E = std::remove_cv_t<std::remove_pointer_t<decltype(src)>>;
+            E* q = reinterpret_cast<E*>(carve(sizeof(E) * len));
+            for (int64_t i = threadIdx.x; i < len; i += NT) q[i] = src[i];
+            return q;
+        };
+        const int32_t nnz = g_rp_a[m];
+        for (int k = 0; k < 5; ++k) sx[k] = stage(gx[k], n);
+        for (int k = 0; k < 4; ++k) sy[k] = stage(gy[k], m);
+        v.cx = sx[0]; v.ix = sx[1]; v.px = sx[2]; v.rx = sx[3]; v.ds = sx[4];
+        v.cy = sy[0]; v.iy = sy[1]; v.py = sy[2]; v.ry = sy[3];
+        v.c = stage(gv.c, n);
+        v.lb = stage(gv.lb, n);
+        v.ub = stage(gv.ub, n);
+        v.clb = stage(gv.clb, m);
+        v.cub = stage(gv.cub, m);
+        rp_t = stage(g_rp_t, n + 1);
+        rp_a = stage(g_rp_a, m + 1);
+        ci_t = stage(g_ci_t, nnz);
+        ci_a = stage(g_ci_a, nnz);
+        v.val_t = stage(gv.val_t, nnz);
+        v.val_a = stage(gv.val_a, nnz);
+        if constexpr (std::is_same<T, double>::value) {  // the FP64 data are these very arrays
+            d.c = v.c;
+            d.lb = v.lb;
+            d.ub = v.ub;
+            d.clb = v.clb;
+            d.cub = v.cub;
+            d.val_t = v.val_t;
+            d.val_a = v.val_a;
+        } else {
+            d.c = stage(gd.c, n);
+            d.lb = stage(gd.lb, n);
+            d.ub = stage(gd.ub, n);
+            d.clb = stage(gd.clb, m);
+            d.cub = stage(gd.cub, m);
+            d.val_t = stage(gd.val_t, nnz);
+            d.val_a = stage(gd.val_a, nnz);
+        }
+        if (gd.row_unscale) d.row_unscale = stage(gd.row_unscale, m);
+        if (gd.col_unscale) d.col_unscale = stage(gd.col_unscale, n);
+        d.dray = reinterpret_cast<double*>(carve(8 * n));  // work vectors: written before read
+        d.yray = reinterpret_cast<double*>(carve(8 * m));
+        __syncthreads();
+    }
     auto evaluate = [&](int32_t which, int32_t phase) {
         double ac[8], ar[4];
 #pragma unroll
@@ -322,6 +396,13 @@ __global__ void __launch_bounds__(kTinyThreads)
         __syncthreads();
         if (!go) break;
     }
+    if constexpr (STAGED) {  // the iterates back to global memory
+        __syncthreads();
+        for (int k = 0; k < 5; ++k)
+            for (int32_t i = threadIdx.x; i < n; i += NT) gx[k][i] = sx[k][i];
+        for (int k = 0; k < 4; ++k)
+            for (int32_t i = threadIdx.x; i < m; i += NT) gy[k][i] = sy[k][i];
+    }
 }
 
 __global__ void lp_begin_kernel(InstState* st) { st[0].t_start_ns = globaltimer_ns(); }
@@ -340,6 +421,7 @@ class LpSolver {
         int dev = 0;
         PDFP_CK(cudaGetDevice(&dev));
         PDFP_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+        PDFP_CK(cudaDeviceGetAttribute(&max_smem_, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         PDFP_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         static const int32_t zero_rp = 0;
         ProblemIn in{A.m, A.n, A.m > 0 ? A.row_ptr : &zero_rp, A.col_idx, A.val, nullptr};
@@ -361,9 +443,14 @@ class LpSolver {
         m_ = A.m;
         n_ = A.n;
         const int e = f32_ ? 4 : 8;
-        it_t_ = M_.make_tiling(ar_, true, StageGeom{e, e, e, 5, 1, 24 * 1024, 2048});
-        it_a_ = M_.make_tiling(ar_, false, StageGeom{e, e, e, 4, 1, 24 * 1024, 2048});
-        if (f32_) {  // FP64 tilings for the polish
+        // the step tilings serve the captured window only (a small LP runs
+        // lp_tiny_solve_kernel); the evaluation tilings also serve the power iteration
+        // and the initial norms
+        if (!tiny_) {
+            it_t_ = M_.make_tiling(ar_, true, StageGeom{e, e, e, 5, 1, 24 * 1024, 2048});
+            it_a_ = M_.make_tiling(ar_, false, StageGeom{e, e, e, 4, 1, 24 * 1024, 2048});
+        }
+        if (f32_ && !tiny_) {  // FP64 tilings for the polish
             it64_t_ = M_.make_tiling(ar_, true, StageGeom{8, 8, 8, 5, 1, 24 * 1024, 2048});
             it64_a_ = M_.make_tiling(ar_, false, StageGeom{8, 8, 8, 4, 1, 24 * 1024, 2048});
         }
@@ -471,6 +558,7 @@ class LpSolver {
     bool cupdlpx_, f32_;
     bool tiny_ = false;  // small LP: whole windows in one launch (lp_tiny_solve_kernel)
     int sms_ = 148;
+    int max_smem_ = 232448;  // dynamic shared memory a block may opt into
     int32_t m_ = 0, n_ = 0;
     cudaStream_t stream_ = nullptr;
     DeviceArena ar_;
@@ -568,13 +656,18 @@ template <typename T>
 void LpSolver::launch_tiny_solve() {
     LpVecs<T>* vp = nullptr;
     if constexpr (std::is_same<T, float>::value) vp = &v32_; else vp = &v64_;
-    const size_t smem = sizeof(double) * 2 * static_cast<size_t>(std::max(std::max(n_, m_), 1));
+    const int32_t rowsum_len = 2 * std::max(std::max(n_, m_), 1);
+    const size_t base = sizeof(double) * static_cast<size_t>(rowsum_len);
+    // the staged form when the LP's copy fits next to the row sums (PDFP_TINY_STAGE=0: in place)
+    const char* ts = std::getenv("PDFP_TINY_STAGE");
+    const size_t staged = base + lp_tiny_stage_bytes<T>(n_, m_, M_.L.NNZ, d_.row_unscale != nullptr);
+    const bool stage = !(ts && ts[0] == '0') && staged <= static_cast<size_t>(max_smem_) - 8 * 1024;
+    const size_t smem = stage ? staged : base;
+    auto kern = stage ? lp_tiny_solve_kernel<T, true> : lp_tiny_solve_kernel<T, false>;
     if (smem > 48 * 1024)
-        PDFP_CK(cudaFuncSetAttribute(lp_tiny_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-    lp_tiny_solve_kernel<T><<<1, kTinyThreads, smem, stream_>>>(*vp, d_, st_, flags_, M_.rp_t, M_.ci_t,
-                                                                M_.rp_a, M_.ci_a, n_, m_, err_,
-                                                                cupdlpx_ ? 1 : 0, kLpTinyWindowsPerLaunch);
+        PDFP_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kern<<<1, kTinyThreads, smem, stream_>>>(*vp, d_, st_, flags_, M_.rp_t, M_.ci_t, M_.rp_a, M_.ci_a, n_,
+                                             m_, err_, cupdlpx_ ? 1 : 0, kLpTinyWindowsPerLaunch, rowsum_len);
     PDFP_CK(cudaGetLastError());
 }
 

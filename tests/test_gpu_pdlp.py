@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 import scipy.sparse as sp
 
-from pdfp_b200 import gpu
+from pdfp_b200 import gpu, synthetic
 from pdfp_b200.milp import MILP, num_continuous
 
 pytestmark = pytest.mark.gpu
@@ -71,3 +71,20 @@ def test_config1_root_lp(oracle):
     xg, _, sg, ig, rg = gpu.solve_lp_relaxation(milp, 1e-3, 120.0, True, return_result=True)
     assert sg == so and ig == io
     assert rg["objective_value"] == pytest.approx(ro["objective_value"], rel=1e-8)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_small_lp_staged_equals_unstaged(monkeypatch, precision):
+    """A small LP runs whole windows in one launch, its data copied into shared memory or
+    read in place (PDFP_TINY_STAGE=0): bit-identical solutions and iteration counts, with
+    (markshare-shaped, continuous slacks) and without (p0201-shaped) the cuPDLPx ray passes."""
+    for milp, cupdlpx in [(synthetic.covering_p0201_like(2), False), (synthetic.markshare_like(3), True)]:
+        out = {}
+        for stage in ("1", "0"):
+            monkeypatch.setenv("PDFP_TINY_STAGE", stage)
+            x, ds, status, iters = gpu.solve_lp_relaxation(milp, tolerance=1e-4,
+                                                           cupdlpx_termination=cupdlpx,
+                                                           precision=precision)
+            out[stage] = (x, ds, status, iters)
+        assert out["1"][2] == out["0"][2] and out["1"][3] == out["0"][3]
+        assert np.array_equal(out["1"][0], out["0"][0]) and np.array_equal(out["1"][1], out["0"][1])
