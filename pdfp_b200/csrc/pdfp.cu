@@ -34,6 +34,7 @@ constexpr int NT_EVAL = 256;
 constexpr int64_t kMixedMinNnz = 1 << 18;  // smaller mixed handles compute in FP64
 constexpr int64_t kTinyMaxDim = 4096;      // rows + columns of a member for the one-launch steps
 constexpr int64_t kTinyMaxNnz = 1 << 16;   // nonzeros of a member for the one-launch steps
+constexpr int32_t kHostNanScanMax = 1 << 16;  // vectors up to this length are checked on the host
 
 // ---- per-instance state kernels ---------------------------------------------------
 
@@ -1109,6 +1110,9 @@ Projector::~Projector() {
     pinned_give(flags_h_, sizeof(InstFlags) * (K_ + 1));
     pinned_give(st_h_, sizeof(InstState) * K_);
     pinned_give(nan_seen_h_, sizeof(int32_t));
+    if (host_stage_ev_) cudaEventSynchronize(host_stage_ev_);
+    pinned_give(host_stage_, host_stage_bytes_);
+    if (host_stage_ev_) cudaEventDestroy(host_stage_ev_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1132,9 +1136,27 @@ void Projector::check_instance(int p) const {
 }
 
 // Stage the caller's column vector of instance p (n values) and raise E_INVALID,
-// before anything is written, when it holds a NaN.
+// before anything is written, when it holds a NaN: a short vector is checked on the
+// host (no round trip to the device), a long one on the device.
 void Projector::stage_cols(int p, const double* src, const char* what) {
     const int32_t n = M_.L.col_off[p + 1] - M_.L.col_off[p];
+    if (n <= kHostNanScanMax) {
+        for (int32_t j = 0; j < n; ++j)
+            if (std::isnan(src[j])) throw Error(E_INVALID, std::string("NaN in the ") + what);
+        // through the handle's own page-locked buffer, so that the caller's may be reused
+        // when this returns; its previous copy must have left it first
+        if (!host_stage_) {
+            host_stage_bytes_ = sizeof(double) * static_cast<size_t>(std::max(M_.max_n, 1));
+            host_stage_ = static_cast<double*>(pinned_take(host_stage_bytes_));
+            PDFP_CK(cudaEventCreateWithFlags(&host_stage_ev_, cudaEventDisableTiming));
+        } else {
+            PDFP_CK(cudaEventSynchronize(host_stage_ev_));
+        }
+        std::memcpy(host_stage_, src, sizeof(double) * n);
+        PDFP_CK(cudaMemcpyAsync(stage_, host_stage_, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+        PDFP_CK(cudaEventRecord(host_stage_ev_, stream_));
+        return;
+    }
     PDFP_CK(cudaMemcpyAsync(stage_, src, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
     PDFP_CK(cudaMemsetAsync(nan_seen_, 0, sizeof(int32_t), stream_));
     launch_elem(K_, n, NanScan{stage_, M_.col_off, p, nan_seen_}, stream_);

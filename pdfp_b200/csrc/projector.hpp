@@ -146,6 +146,9 @@ class Projector {
     int32_t* err_ = nullptr;
     SolveParams* sp_ = nullptr;
     double* stage_ = nullptr;
+    double* host_stage_ = nullptr;         // page-locked copy of a short caller vector
+    size_t host_stage_bytes_ = 0;
+    cudaEvent_t host_stage_ev_ = nullptr;  // its last copy to stage_ has left it
     double* col_scale_ = nullptr;  // D_c in packed column order, once set_col_scale ran
     std::vector<bool> has_col_scale_;
     int32_t* nan_seen_ = nullptr;
