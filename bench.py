@@ -358,12 +358,16 @@ def main():
         gpu.L.check(gpu.L.lib().pdfp_get_tuning_reducers(st._h, red))
         tuning["a_t_reducers"] = red[0]
         tuning["a_reducers"] = red[1]
+        seg = (gpu.C.c_int32 * 2)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning_seg(st._h, seg))
+        tuning["a_long_row_segments"] = seg[0]
+        tuning["a_long_row_threshold"] = seg[1]
         tms = (gpu.C.c_float * 256)()
         tcfg = (gpu.C.c_int32 * (7 * 256))()
         cnt = gpu.C.c_int32()
         gpu.L.check(gpu.L.lib().pdfp_get_tuning_table(st._h, tms, tcfg, 256, gpu.C.byref(cnt)))
         for i in range(min(cnt.value, 256)):
-            log(f"[bench]   tune side={'A' if tcfg[7*i] else 'At'} stage={tcfg[7*i+1]} "
+            log(f"[bench]   tune side={['At', 'A', 'A+seg'][tcfg[7*i]]} stage={tcfg[7*i+1]} "
                 f"nt={tcfg[7*i+2]} l2={tcfg[7*i+3]} stages={tcfg[7*i+4]} cap={tcfg[7*i+5]} "
                 f"red={tcfg[7*i+6]}: {tms[i]*1e3:.1f} us")
         log(f"[bench] {precision} handle built in {time.time() - t:.1f}s, tuning {tuning}")
@@ -433,26 +437,43 @@ def main():
     if mx["kp_ms"] and mx["kd_ms"]:
         # one entry per step kernel; `roofline` is the one that takes longer per launch
         bytes_dual32 = 8.0 * nnz + 4.0 * (m + 1) + 4.0 * 4 * m + 4.0 * n
-        # DRAM bytes of one launch on the default workload, from ncu captures
+        # DRAM bytes of one launch on the default workload, by engine, from ncu captures
         # (dram__bytes_read.sum + dram__bytes_write.sum)
         default = (args.workload, args.m, args.n, args.nnz) == ("zipf-lp", 1_000_000, 2_000_000,
                                                                 20_000_000)
+        traffic_ncu = {("PrimalOp", "tile"): 242.8e6, ("DualOp", "tile"): 187.9e6}
         tun = mx["tuning"]
 
+        seg = tun.get("a_long_row_segments", 0)
+
+        def engine(op, threads):
+            if op == "DualOp" and seg:
+                return "tile+seg"
+            return "flat" if threads == 0 else "vec" if threads == 32 else "tile"
+
         def kname(op, threads):
-            return (f"flat_spmv_kernel<{op}<float, false, 256>>" if threads == 0
-                    else f"tile_spmv_kernel<{op}<float, false, {threads}>>")
+            if threads == 0:
+                return f"flat_spmv_kernel<{op}<float, false, 256>>"
+            if threads == 32:
+                return f"vec_spmv_kernel<{op}<float, false, 256>>"
+            name = f"tile_spmv_kernel<{op}<float, false, {threads}>>"
+            if op == "DualOp" and seg:  # the A side in three launches
+                name = (f"seg_partials_kernel<{op}<float, false, 256>> + seg_finish_kernel + "
+                        f"{name} [rows of >= {tun['a_long_row_threshold']} nonzeros in "
+                        f"{seg} column segments]")
+            return name
 
         entries = []
-        for label, op, threads, ms, byts, traffic in [
+        for label, op, threads, ms, byts in [
                 ("A'z + fused primal/y update", "PrimalOp", tun["a_t_threads"], mx["kp_ms"],
-                 bytes_primal32, 242.8e6),
+                 bytes_primal32),
                 ("A x_bar + fused z update", "DualOp", tun["a_threads"], mx["kd_ms"],
-                 bytes_dual32, 187.9e6)]:
+                 bytes_dual32)]:
             achieved = byts / (ms * 1e-3) / 1e9
+            traffic = traffic_ncu.get((op, engine(op, threads))) if default else None
             entries.append({"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                             "unit": "GB/s", "frac": round(achieved / peak, 4),
-                            "traffic": traffic if default else None,
+                            "traffic": traffic,
                             "kernel": f"{kname(op, threads)} ({label})", "peak_kind": peak_kind,
                             "bytes_per_launch": byts, "mean_launch_ms": round(ms, 5)})
         entries.sort(key=lambda e: -e["mean_launch_ms"])

@@ -235,18 +235,22 @@ PDFP_API int pdfp_set_polish(pdfp_handle* h, int32_t stall_evaluations, double f
  * in L2 only, 2 = per-thread async copies into the shared-memory stage (FP32
  * steps of the tile engine; the reducers form the products, with the same
  * roundings in the same order, so results do not depend on the policy).
+ * The FP32 steps may also run on the vec engine (warps over rows read straight
+ * from the CSR arrays, lanes per row by row length; threads per role 32, "stage
+ * bytes" its target nonzeros per lane 1, 2, 4 or 8; gather policy 0 or 1).
  * PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size, and
- * PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the engine with its default
- * settings (flat1: the flat engine's one-quad-per-thread variant), and
+ * PDFP_STEP_ENGINE=tile / =flat / =flat1 / =vec fixes the engine with its default
+ * settings (flat1: the flat engine's one-quad-per-thread variant; vec: the FP32
+ * steps, the FP64 steps stay on the tile engine), and
  * PDFP_TUNING="s,t,l,s,t,l[,n,n[,b,b]]" pins both sides for handles created
  * while it is set: stage bytes, threads per role and the gather policy of A',
  * then of A, with the values out[] below reports, and optionally the stage
  * counts of A' and A (pdfp_get_tuning_stages; default 4), their caps on
  * resident blocks per SM (pdfp_get_tuning_blocks; default 0) and their reducer
  * threads (pdfp_get_tuning_reducers; 0: as many as gatherers).
- * out[8] = {A' stage bytes, A' threads per role (0: flat engine), A' tiles,
- * A stage bytes, A threads per role (0: flat engine), A tiles,
- * A' gather policy, A gather policy}. */
+ * out[8] = {A' stage bytes, A' threads per role (0: flat engine, 32: vec
+ * engine), A' tiles (vec engine: work items), A stage bytes, A threads per role,
+ * A tiles, A' gather policy, A gather policy}. */
 PDFP_API int pdfp_get_tuning(const pdfp_handle* h, int32_t* out);
 /* Shared-memory stages per block of the tile engine on each side: out[2] =
  * {A', A} (2..4; 4 for the flat engine, which has none). */
@@ -260,10 +264,24 @@ PDFP_API int pdfp_get_tuning_blocks(const pdfp_handle* h, int32_t* out);
  * (the gatherers are the threads per role of pdfp_get_tuning; FP32 steps may run
  * half as many reducers as gatherers; 0 for the flat engine). */
 PDFP_API int pdfp_get_tuning_reducers(const pdfp_handle* h, int32_t* out);
+/* The A-side step of the FP32 steps with its long rows regrouped by column
+ * segment: out[2] = {segments, long-row threshold in nonzeros}, {0, 0} when the
+ * handle runs it without.  The rows with at least that many nonzeros are summed
+ * by one block per column segment, gathering from that segment of x_bar held in
+ * shared memory, and finished one warp per row (FP64 sum of the segments'
+ * partials in segment order); the other rows stay on the tile engine.  The
+ * autotuner tries a few segmentations on handles of at least 2^22 nonzeros
+ * and keeps one only if it beats the tile engine's A-side step.  PDFP_SEG=0
+ * switches this off; PDFP_SEG="n,l[,s,t,k]" fixes n segments and threshold l
+ * (and the partials pass's stage bytes, threads per role and stages). */
+PDFP_API int pdfp_get_tuning_seg(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
  * launch time, cfg[7i..7i+6] = {side (0: A', 1: A), stage bytes, gatherer
- * threads (0: flat engine), gather policy, stages, blocks per SM cap, reducer
- * threads}; *count receives the number of rows. */
+ * threads (0: flat engine; 32: vec engine, whose stage bytes are its nonzeros
+ * per lane), gather policy, stages, blocks per SM cap, reducer threads}; side 2:
+ * the A side with segmented long rows (pdfp_get_tuning_seg), {2, segments,
+ * long-row threshold, gather policy of the other rows, then the partials pass's
+ * stages, stage bytes and threads per role}; *count receives the number of rows. */
 PDFP_API int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
                                    int32_t* count);
 

@@ -161,19 +161,17 @@ void DeviceMatrix::refresh_f32(cudaStream_t s) {
     PDFP_CK(cudaGetLastError());
 }
 
-DeviceMatrix::Tiling DeviceMatrix::make_tiling(DeviceArena& ar, bool transpose,
-                                               const StageGeom& g) const {
-    Tiling t;
-    const HostCsr& csr = transpose ? L.At : L.A;
-    build_tiling(csr, transpose ? L.col_off : L.row_off, g, t.host);
+// Upload a built tiling of the CSR whose device arrays are rp / ci.
+static DeviceMatrix::Tiling upload_tiling(DeviceArena& ar, DeviceMatrix::Tiling&& t, int32_t rows,
+                                          const int32_t* rp, const int32_t* ci, const StageGeom& g) {
     SideDev& s = t.dev;
-    s.rows = csr.rows;
+    s.rows = rows;
     s.n_tiles = static_cast<int32_t>(t.host.tile_inst.size());
     s.n_chunks = static_cast<int32_t>(t.host.chunk_k0.size());
     s.max_tile_rows = t.host.max_tile_rows;
     s.stage_bytes = g.stage_bytes;
-    s.rp = transpose ? rp_t : rp_a;
-    s.ci = transpose ? ci_t : ci_a;
+    s.rp = rp;
+    s.ci = ci;
     s.tile_row = ar.upload(t.host.tile_row);
     s.tile_chunk = ar.upload(t.host.tile_chunk);
     s.tile_inst = ar.upload(t.host.tile_inst);
@@ -181,12 +179,65 @@ DeviceMatrix::Tiling DeviceMatrix::make_tiling(DeviceArena& ar, bool transpose,
     for (size_t c = 0; c < desc.size(); ++c) {
         const int32_t tile = t.host.chunk_tile[c];
         desc[c] = ChunkDesc{t.host.chunk_k0[c], t.host.chunk_k1[c], t.host.tile_row[tile],
-                            t.host.tile_row[tile + 1], tile, t.host.tile_inst[tile],
+                            t.host.tile_row_end[tile], tile, t.host.tile_inst[tile],
                             t.host.chunk_flags[c], t.host.tile_chunk[tile] == (int32_t)c ? 1 : 0};
     }
     s.chunks = ar.upload(desc);
     t.inst_tile0 = ar.upload(t.host.inst_tile0);
-    return t;
+    return std::move(t);
+}
+
+DeviceMatrix::Tiling DeviceMatrix::make_tiling(DeviceArena& ar, bool transpose,
+                                               const StageGeom& g,
+                                               const std::vector<uint8_t>* skip) const {
+    Tiling t;
+    const HostCsr& csr = transpose ? L.At : L.A;
+    build_tiling(csr, transpose ? L.col_off : L.row_off, g, t.host, skip);
+    return upload_tiling(ar, std::move(t), csr.rows, transpose ? rp_t : rp_a, transpose ? ci_t : ci_a, g);
+}
+
+bool DeviceMatrix::make_seg(DeviceArena& ar, int nseg, int long_min, const StageGeom& g,
+                            SegDev& d, Tiling& pairs, std::vector<uint8_t>& is_long) const {
+    HostSeg h;
+    if (!build_seg(L.A, L.row_off, nseg, long_min, h)) return false;
+    const int64_t nl = static_cast<int64_t>(h.long_row.size());
+    d = SegDev();
+    d.nseg = h.nseg;
+    d.seg_len = h.seg_len;
+    d.n_cols = h.n_cols;
+    d.n_long = static_cast<int32_t>(nl);
+    d.long_row = ar.upload(h.long_row);
+    d.long_inst = ar.upload(h.long_inst);
+    std::vector<float> v32(h.pairs.v.size());
+    for (size_t k = 0; k < v32.size(); ++k) v32[k] = static_cast<float>(h.pairs.v[k]);  // as refresh_f32 rounds
+    d.val = ar.upload(v32);
+    d.partial = ar.alloc<float>(static_cast<size_t>(nl) * nseg);
+    // tiles of the pairs, the segments as instances, interleaved one block per segment
+    std::vector<int32_t> off(nseg + 1);
+    for (int s = 0; s <= nseg; ++s) off[s] = static_cast<int32_t>(s * nl);
+    HostTiling by_seg;
+    build_tiling(h.pairs, off, g, by_seg);
+    Tiling t;
+    interleave_tiles(by_seg, nseg, t.host);
+    const int32_t* rp = ar.upload(h.pairs.rp);
+    const int32_t* ci = ar.upload(h.pairs.ci);
+    pairs = upload_tiling(ar, std::move(t), h.pairs.rows, rp, ci, g);
+    is_long.swap(h.is_long);
+    return true;
+}
+
+VecDev DeviceMatrix::make_vec(DeviceArena& ar, bool transpose, int lane_nnz) const {
+    const HostCsr& csr = transpose ? L.At : L.A;
+    std::vector<VecItem> items;
+    const int32_t slots = build_vec_items(csr, transpose ? L.col_off : L.row_off, lane_nnz, items);
+    VecDev v;
+    v.n_items = static_cast<int32_t>(items.size());
+    v.rp = transpose ? rp_t : rp_a;
+    v.ci = transpose ? ci_t : ci_a;
+    v.items = ar.upload(items);
+    v.piece_sum = ar.alloc<double>(slots > 0 ? slots : 1);  // zero-filled
+    v.piece_cnt = ar.alloc<int32_t>(slots > 0 ? slots : 1);
+    return v;
 }
 
 }  // namespace pdfp

@@ -135,8 +135,19 @@ class DeviceMatrix {
         SideDev dev{};
         int32_t* inst_tile0 = nullptr;  // device copy, K + 1
     };
-    // Build and upload a tiling of A (transpose = false) or A'.
-    Tiling make_tiling(DeviceArena& ar, bool transpose, const StageGeom& g) const;
+    // Build and upload a tiling of A (transpose = false) or A', leaving out the
+    // rows `skip` marks (build_tiling).
+    Tiling make_tiling(DeviceArena& ar, bool transpose, const StageGeom& g,
+                       const std::vector<uint8_t>* skip = nullptr) const;
+    // Build and upload the vec engine's items of A (transpose = false) or A'
+    // (build_vec_items), with zeroed piece slots and counters.
+    VecDev make_vec(DeviceArena& ar, bool transpose, int lane_nnz) const;
+    // Build and upload A's long rows by column segment (build_seg) and a tiling of
+    // their (segment, long row) pairs in stage geometry g, interleaved one block per
+    // segment (interleave_tiles); false when no row qualifies.  `is_long` receives
+    // the rows it took (for the tiling of the rest).
+    bool make_seg(DeviceArena& ar, int nseg, int long_min, const StageGeom& g, SegDev& out,
+                  Tiling& pairs, std::vector<uint8_t>& is_long) const;
 };
 
 }  // namespace pdfp

@@ -10,6 +10,8 @@
 #include "state.hpp"
 #include "flat_spmv.cuh"
 #include "tile_spmv.cuh"
+#include "vec_spmv.cuh"
+#include "seg_spmv.cuh"
 
 namespace pdfp {
 
@@ -64,6 +66,7 @@ void launch_tile_k(const SideDev& s, const Op& op, int grid, cudaStream_t stream
     cfg.gridDim = dim3(static_cast<unsigned>(grid));
     cfg.blockDim = dim3(Op::NT + NR + 32);
     cfg.dynamicSmemBytes = tile_dyn_smem<Op>(s);
+    if constexpr (HasPrologue<Op>::value) cfg.dynamicSmemBytes += op.extra_smem();
     cfg.stream = stream;
     cudaLaunchAttribute at[2];
     int na = 0;
@@ -135,6 +138,75 @@ void launch_flat(const SideDev& s, const Op& op, int qpt, int grid, cudaStream_t
         flat_spmv_kernel<Op, 1><<<grid, kFlatThreads, 0, stream>>>(s, op);
     else
         flat_spmv_kernel<Op, 2><<<grid, kFlatThreads, 0, stream>>>(s, op);
+}
+
+// ---- launching the vec engine -----------------------------------------------------
+
+// Blocks resident on all SMs, no more than the items need (8 warps per block).
+template <class Op>
+int vec_grid(const VecDev& s, int num_sms) {
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vec_spmv_kernel<Op>, kVecThreads, 0);
+    const int g = (blocks > 0 ? blocks : 1) * num_sms;
+    const int need = (s.n_items + kVecThreads / 32 - 1) / (kVecThreads / 32);
+    return g < need ? g : need;
+}
+
+template <class Op>
+void launch_vec(const VecDev& s, const Op& op, int grid, cudaStream_t stream) {
+    if (s.n_items <= 0 || grid <= 0) return;
+    vec_spmv_kernel<Op><<<grid, kVecThreads, 0, stream>>>(s, op);
+}
+
+// ---- launching the segmented long rows ------------------------------------------
+
+template <int NT, class DOp>
+SegPartialOp<NT> seg_partial_op(const SideDev& pairs, const SegDev& g, const DOp& dop) {
+    SegPartialOp<NT> op{};
+    op.x = dop.v.rx;  // x_bar, which the A-side step gathers
+    op.vals = g.val;
+    op.partial = g.partial;
+    op.nseg = g.nseg;
+    op.seg_len = g.seg_len;
+    op.n_cols = g.n_cols;
+    op.n_long = g.n_long;
+    op.xs_off = static_cast<uint32_t>(tile_dyn_smem<SegPartialOp<NT>>(pairs));
+    op.errp = dop.errp;
+    return op;
+}
+
+// Raises the partials kernel's shared-memory limit for this tiling; false when a
+// block cannot have that much.
+template <int NT, class DOp>
+bool seg_attr(const SideDev& pairs, const SegDev& g, const DOp& dop, int max_smem_optin) {
+    using SOp = SegPartialOp<NT>;
+    const SOp op = seg_partial_op<NT>(pairs, g, dop);
+    const size_t smem = tile_dyn_smem<SOp>(pairs) + op.extra_smem();
+    if (smem > static_cast<size_t>(max_smem_optin)) return false;
+    static size_t attr = 0;  // per kernel: only ever raised
+    if (smem > attr) {
+        if (cudaFuncSetAttribute(tile_spmv_kernel<SOp, false, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)) != cudaSuccess)
+            return false;
+        attr = smem;
+    }
+    return true;
+}
+
+// The long rows' partials (bps blocks per segment) and their finish.
+template <class DOp>
+void launch_seg(const SideDev& pairs, const SegDev& g, int nt, int bps, const DOp& dop,
+                cudaStream_t stream) {
+    if (g.n_long <= 0 || g.nseg <= 0) return;
+    const int grid = g.nseg * bps;
+    if (nt == 256)
+        launch_tile_k<SegPartialOp<256>, false, 256>(pairs, seg_partial_op<256>(pairs, g, dop), grid,
+                                                     stream, false, -1);
+    else
+        launch_tile_k<SegPartialOp<128>, false, 128>(pairs, seg_partial_op<128>(pairs, g, dop), grid,
+                                                     stream, false, -1);
+    const unsigned blocks = static_cast<unsigned>((g.n_long + 31) / 32);
+    seg_finish_kernel<DOp><<<blocks, 32 * kSegFinWarps, 0, stream>>>(g, dop);
 }
 
 // ---- per-tile elementwise reductions and per-instance finalisation ---------------

@@ -9,12 +9,13 @@
 namespace pdfp {
 
 void build_tiling(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
-                  const StageGeom& g, HostTiling& t) {
+                  const StageGeom& g, HostTiling& t, const std::vector<uint8_t>* skip) {
     t = HostTiling();
     t.geom = g;
     const int K = static_cast<int>(inst_row_off.size()) - 1;
     const std::vector<int32_t>& rp = csr.rp;
-    t.tile_row.push_back(0);
+    auto skipped = [&](int32_t r) { return skip && (*skip)[r] != 0; };
+    std::vector<int32_t> starts;
     t.tile_chunk.push_back(0);
     t.inst_tile0.push_back(0);
     int32_t max_rows = 1;
@@ -22,7 +23,12 @@ void build_tiling(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
         int32_t r = inst_row_off[p];
         const int32_t rend = inst_row_off[p + 1];
         while (r < rend) {
+            if (skipped(r)) {
+                ++r;
+                continue;
+            }
             const int32_t tile = static_cast<int32_t>(t.tile_inst.size());
+            starts.push_back(r);
             if (chunk_stage_bytes(g, rp[r], rp[r + 1], r, r + 1, true, false) >
                 static_cast<uint32_t>(g.stage_bytes)) {
                 // a long row: one tile, several chunks
@@ -43,7 +49,7 @@ void build_tiling(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
                 r += 1;
             } else {
                 int32_t r1 = r + 1;
-                while (r1 < rend && (r1 + 1 - r) <= g.max_rows &&
+                while (r1 < rend && !skipped(r1) && (r1 + 1 - r) <= g.max_rows &&
                        chunk_stage_bytes(g, rp[r], rp[r1 + 1], r, r1 + 1, true, false) <=
                            static_cast<uint32_t>(g.stage_bytes))
                     ++r1;
@@ -55,12 +61,149 @@ void build_tiling(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
                 r = r1;
             }
             t.tile_inst.push_back(p);
-            t.tile_row.push_back(r);
+            t.tile_row_end.push_back(r);
             t.tile_chunk.push_back(static_cast<int32_t>(t.chunk_k0.size()));
         }
         t.inst_tile0.push_back(static_cast<int32_t>(t.tile_inst.size()));
     }
+    // tile t covers rows [tile_row[t], tile_row_end[t]); without skipped rows the
+    // tiles are contiguous and tile_row[t + 1] == tile_row_end[t]
+    t.tile_row = starts;
+    t.tile_row.push_back(t.tile_row_end.empty() ? (K > 0 ? inst_row_off[K] : 0) : t.tile_row_end.back());
     t.max_tile_rows = max_rows;
+}
+
+int32_t build_vec_items(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
+                        int lane_nnz, std::vector<VecItem>& items) {
+    items.clear();
+    const int K = static_cast<int>(inst_row_off.size()) - 1;
+    const std::vector<int32_t>& rp = csr.rp;
+    const int rpg = std::max(1, 8 / std::max(1, lane_nnz));
+    auto lanes_log2 = [&](int64_t len) {
+        int lg = 0;
+        while (lg < 5 && (int64_t(1) << lg) * lane_nnz < len) ++lg;
+        return lg;
+    };
+    std::vector<VecItem> pieces;
+    int32_t slots = 0;
+    for (int p = 0; p < K; ++p) {
+        int32_t r = inst_row_off[p];
+        const int32_t rend = inst_row_off[p + 1];
+        while (r < rend) {
+            const int64_t len = rp[r + 1] - rp[r];
+            if (len > kVecPiece) {
+                const int32_t np = static_cast<int32_t>((len + kVecPiece - 1) / kVecPiece);
+                for (int32_t q = 0; q < np; ++q) {
+                    const int32_t k0 = rp[r] + q * kVecPiece;
+                    const int32_t k1 = std::min<int32_t>(k0 + kVecPiece, rp[r + 1]);
+                    pieces.push_back(VecItem{r, slots, p, -1, k0, k1, slots + q, np});
+                }
+                slots += np;
+                ++r;
+                continue;
+            }
+            const int lg = lanes_log2(len);
+            int32_t cap = (32 >> lg) * rpg;
+            while (cap > (32 >> lg) && static_cast<int64_t>(cap) * len > 2048) cap -= 32 >> lg;
+            int32_t r1 = r + 1;
+            while (r1 < rend && r1 - r < cap) {
+                const int64_t l1 = rp[r1 + 1] - rp[r1];
+                if (l1 > kVecPiece || lanes_log2(l1) != lg) break;
+                ++r1;
+            }
+            items.push_back(VecItem{r, r1, p, lg, 0, 0, 0, 0});
+            r = r1;
+        }
+    }
+    std::stable_sort(items.begin(), items.end(),
+                     [](const VecItem& a, const VecItem& b) { return a.lg > b.lg; });
+    items.insert(items.begin(), pieces.begin(), pieces.end());
+    return slots;
+}
+
+bool build_seg(const HostCsr& csr, const std::vector<int32_t>& inst_row_off, int nseg,
+               int long_min, HostSeg& o) {
+    o = HostSeg();
+    const int K = static_cast<int>(inst_row_off.size()) - 1;
+    const int64_t ncols = csr.cols;
+    if (nseg <= 0 || ncols <= 0 || K <= 0 || long_min <= 0) return false;
+    // a multiple of 4, so that each segment of an FP32 vector starts 16-byte aligned
+    const int64_t seg_len = ((ncols + nseg - 1) / nseg + 3) & ~int64_t(3);
+    if (seg_len > 65536) return false;
+    const std::vector<int32_t>& rp = csr.rp;
+    const std::vector<int32_t>& ci = csr.ci;
+    o.is_long.assign(csr.rows, 0);
+    for (int p = 0; p < K; ++p)
+        for (int32_t r = inst_row_off[p]; r < inst_row_off[p + 1]; ++r) {
+            if (rp[r + 1] - rp[r] < long_min) continue;
+            o.is_long[r] = 1;
+            o.long_row.push_back(r);
+            o.long_inst.push_back(p);
+        }
+    const int64_t nl = static_cast<int64_t>(o.long_row.size());
+    if (nl == 0 || static_cast<int64_t>(nseg) * nl > 0x7ffffff0LL) {
+        o = HostSeg();
+        return false;
+    }
+    o.nseg = nseg;
+    o.seg_len = static_cast<int32_t>(seg_len);
+    o.n_cols = static_cast<int32_t>(ncols);
+    HostCsr& P = o.pairs;
+    P.rows = static_cast<int32_t>(nseg * nl);
+    P.cols = static_cast<int32_t>(seg_len);
+    P.rp.assign(static_cast<size_t>(P.rows) + 1, 0);
+    for (int64_t q = 0; q < nl; ++q) {
+        const int32_t r = o.long_row[q];
+        for (int32_t k = rp[r]; k < rp[r + 1]; ++k) ++P.rp[static_cast<size_t>(ci[k] / seg_len) * nl + q + 1];
+    }
+    for (size_t i = 1; i < P.rp.size(); ++i) P.rp[i] += P.rp[i - 1];
+    P.ci.resize(P.rp.back());
+    P.v.resize(P.rp.back());
+    std::vector<int32_t> cur(nseg);
+    for (int64_t q = 0; q < nl; ++q) {
+        const int32_t r = o.long_row[q];
+        for (int s = 0; s < nseg; ++s) cur[s] = P.rp[s * nl + q];
+        for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
+            const int32_t s = static_cast<int32_t>(ci[k] / seg_len);
+            const int32_t e = cur[s]++;
+            P.ci[e] = static_cast<int32_t>(ci[k] - s * seg_len);
+            P.v[e] = csr.v[k];
+        }
+    }
+    return true;
+}
+
+void interleave_tiles(const HostTiling& in, int nseg, HostTiling& t) {
+    t = HostTiling();
+    t.geom = in.geom;
+    t.max_tile_rows = in.max_tile_rows;
+    int32_t most = 0;
+    for (int s = 0; s < nseg; ++s) most = std::max(most, in.inst_tile0[s + 1] - in.inst_tile0[s]);
+    t.tile_chunk.push_back(0);
+    for (int32_t j = 0; j < most; ++j)
+        for (int s = 0; s < nseg; ++s) {
+            const int32_t tile = static_cast<int32_t>(t.tile_inst.size());
+            const int32_t src = in.inst_tile0[s] + j;
+            if (src < in.inst_tile0[s + 1]) {
+                t.tile_row.push_back(in.tile_row[src]);
+                t.tile_row_end.push_back(in.tile_row_end[src]);
+                t.tile_inst.push_back(s);
+                for (int32_t c = in.tile_chunk[src]; c < in.tile_chunk[src + 1]; ++c) {
+                    t.chunk_k0.push_back(in.chunk_k0[c]);
+                    t.chunk_k1.push_back(in.chunk_k1[c]);
+                    t.chunk_tile.push_back(tile);
+                    t.chunk_flags.push_back(in.chunk_flags[c]);
+                }
+            } else {  // padding: no rows, no chunks
+                t.tile_row.push_back(0);
+                t.tile_row_end.push_back(0);
+                t.tile_inst.push_back(-1);
+            }
+            t.tile_chunk.push_back(static_cast<int32_t>(t.chunk_k0.size()));
+        }
+    t.tile_row.push_back(in.tile_row.empty() ? 0 : in.tile_row.back());
+    t.inst_tile0.assign(1, 0);
+    t.inst_tile0.push_back(static_cast<int32_t>(t.tile_inst.size()));
 }
 
 std::string build_layout(const std::vector<ProblemIn>& probs, bool permute, HostLayout& L) {

@@ -118,13 +118,17 @@ struct HostCsr {
 struct HostTiling {
     std::vector<int32_t> tile_row, tile_chunk, tile_inst, chunk_k0, chunk_k1, chunk_tile,
         chunk_flags;
+    std::vector<int32_t> tile_row_end;  // n_tiles: one past each tile's last row
     std::vector<int32_t> inst_tile0;  // K + 1: tiles of instance p are [inst_tile0[p], inst_tile0[p+1])
     int32_t max_tile_rows = 1;
     StageGeom geom{};
 };
 
+// Tiles of whole rows in row order; rows with (*skip)[r] != 0 are left out (their
+// neighbours then fall in different tiles, so only the tile engine, which reads
+// each chunk's row range, may run a tiling with skipped rows).
 void build_tiling(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
-                  const StageGeom& g, HostTiling& t);
+                  const StageGeom& g, HostTiling& t, const std::vector<uint8_t>* skip = nullptr);
 
 // Caps of the flat step engine (flat_spmv.cuh): a multi-row tile holds at most
 // kFlatMaxRows rows and its nonzeros, counted from the 4-aligned element below
@@ -151,6 +155,71 @@ inline bool flat_tiling_fits(const HostTiling& t, int cap) {
     }
     return true;
 }
+
+// Work items of the vec step engine (vec_spmv.cuh), one warp each.  lg >= 0:
+// rows [r0, r1) of instance `inst` with 2^lg lanes per row.  lg = -1: the
+// nonzeros [k0, k1) of long row r0, piece `slot - r1` of its `np` pieces, whose
+// FP64 partial sums occupy slots [r1, r1 + np) (slot r1 also indexes the row's
+// completion counter).
+struct alignas(32) VecItem {
+    int32_t r0, r1, inst, lg, k0, k1, slot, np;
+};
+
+constexpr int kVecPiece = 1024;  // nonzeros per piece of a long row
+
+// Device view of one side of the matrix as vec-engine items.
+struct VecDev {
+    int32_t n_items = 0;
+    const int32_t* rp = nullptr;
+    const int32_t* ci = nullptr;
+    const VecItem* items = nullptr;
+    double* piece_sum = nullptr;  // n_slots
+    int32_t* piece_cnt = nullptr;  // n_slots, all zero between launches
+};
+
+// Items of one side: rows longer than kVecPiece are cut into pieces; the other
+// rows get the lanes per row that give each lane about `lane_nnz` nonzeros (a
+// power of two up to 32), and runs of rows with equal lanes are cut into items
+// of (32 / lanes) x max(1, 8 / lane_nnz) rows, fewer where the item would hold
+// more than 2048 nonzeros.  Items are ordered longest-first: pieces, then by
+// decreasing lanes per row, each group in row order.  Returns the slot count.
+int32_t build_vec_items(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
+                        int lane_nnz, std::vector<VecItem>& items);
+
+// The long rows of A by column segment (seg_spmv.cuh).  The packed columns are cut
+// into nseg segments of seg_len (a multiple of 4; the last segments may be short
+// or empty); each long row's nonzeros are regrouped segment by
+// segment into a CSR whose rows are the (segment, long row) pairs, segment-major
+// (row s * n_long + q holds long row q's entries in segment s, in the row's
+// storage order), with column indices relative to the segment start.  One block
+// per segment, holding that segment of the gathered vector in shared memory,
+// forms every pair's sum: the long row's partial for the segment.
+struct SegDev {
+    int32_t nseg = 0, seg_len = 0, n_cols = 0, n_long = 0;
+    const int32_t* long_row = nullptr;   // n_long: packed row index of each long row
+    const int32_t* long_inst = nullptr;  // n_long: its instance
+    const float* val = nullptr;          // the regrouped entries' values (FP32)
+    float* partial = nullptr;            // nseg x n_long partial sums (pair order)
+};
+
+struct HostSeg {
+    int32_t nseg = 0, seg_len = 0, n_cols = 0;
+    std::vector<int32_t> long_row, long_inst;
+    HostCsr pairs;                 // rows: the pairs; ci: column - segment start; v: values
+    std::vector<uint8_t> is_long;  // per row of A: 1 for the long rows
+};
+
+// Long rows: at least `long_min` nonzeros.  Returns false (and leaves `out` empty)
+// when no row qualifies or a segment would span more than 65,536 columns.
+bool build_seg(const HostCsr& csr, const std::vector<int32_t>& inst_row_off, int nseg,
+               int long_min, HostSeg& out);
+
+// The tiles of a tiling whose instances are the segments (tiles of segment s are
+// [inst_tile0[s], inst_tile0[s+1])), reordered so that tile j * nseg + s is the
+// j-th tile of segment s: a grid of nseg blocks walking tiles b, b + nseg, ...
+// then gives block s exactly the tiles of segment s.  Segments with fewer tiles
+// are padded with empty tiles of instance -1.
+void interleave_tiles(const HostTiling& in, int nseg, HostTiling& out);
 
 // One problem as handed to the library (CSR, caller's numbering).
 struct ProblemIn {

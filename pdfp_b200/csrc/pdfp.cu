@@ -597,6 +597,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     PDFP_CK(cudaGetDevice(&dev));
     PDFP_CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
     PDFP_CK(cudaDeviceGetAttribute(&max_smem_sm_, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    PDFP_CK(cudaDeviceGetAttribute(&max_smem_block_, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     PDFP_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     std::vector<ProblemIn> in;
     for (const ProblemData& p : probs)
@@ -774,8 +775,9 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     // The autotuner pays for itself only where a step kernel takes longer than its
     // launch: below 256K nonzeros every candidate times the same few microseconds.
     // PDFP_AUTOTUNE=0 / =1 switches it off / on regardless of size.
-    // PDFP_STEP_ENGINE=tile / =flat / =flat1 fixes the step engine (flat1: one quad
-    // per thread and tile) and skips the tuner.
+    // PDFP_STEP_ENGINE=tile / =flat / =flat1 / =vec fixes the step engine (flat1: one
+    // quad per thread and tile; vec: the FP32 steps only, the FP64 steps keep the
+    // tile engine) and skips the tuner.
     // The step kernels stream the matrix under an L2 evict-first policy, so the
     // gathered vector and the iterates stay in L2 (zipf-lp: 1% more iterations/s);
     // PDFP_STREAM_EVICT_FIRST=0 / =1 switches it off / on.
@@ -789,17 +791,52 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     const char* se = std::getenv("PDFP_STEP_ENGINE");
     const int forced = !se ? -1
                        : std::strcmp(se, "tile") == 0 ? 0
-                       : std::strcmp(se, "flat") == 0 || std::strcmp(se, "flat1") == 0 ? 1 : -1;
+                       : std::strcmp(se, "flat") == 0 || std::strcmp(se, "flat1") == 0 ? 1
+                       : std::strcmp(se, "vec") == 0 ? 2 : -1;
     if (forced >= 0) {
         const int qpt = std::strcmp(se, "flat1") == 0 ? 1 : 2;
         for (StepSide* q : {&p32_, &d32_, &p64_, &d64_}) {
+            if (forced == 2 && (q == &p64_ || q == &d64_)) continue;
             q->engine = forced;
             q->qpt = qpt;
         }
     }
+    // PDFP_SEG=0 keeps the A side's long rows on the step engine; PDFP_SEG="n,l"
+    // regroups the rows of at least l nonzeros into n column segments (seg_spmv.cuh)
+    // whenever the FP32 A side runs on the tile engine; unset, the autotuner tries
+    // a few such forms against the plain tile engine.
+    // Optional after them: the partials' stage bytes, threads per role and stages.
+    if (const char* sg = std::getenv("PDFP_SEG")) {
+        int n = 0, l = 0, sb = d32_.seg_stage, nt = d32_.seg_nt, ns = d32_.seg_stages, bps = 1;
+        const int got = std::sscanf(sg, "%d,%d,%d,%d,%d,%d", &n, &l, &sb, &nt, &ns, &bps);
+        if (got == 1 && n == 0) {
+            seg_mode_ = 0;
+        } else if ((got == 2 || got == 5 || got == 6) && n > 0 && n <= 65536 && l > 0 &&
+                   sb >= 8192 && sb <= 49152 && sb % 128 == 0 && (nt == 128 || nt == 256) &&
+                   ns >= 2 && ns <= 4 && bps >= 1 && bps <= 8) {
+            seg_mode_ = n;
+            seg_long_ = l;
+            seg_cfg_[0] = sb;
+            seg_cfg_[1] = nt;
+            seg_cfg_[2] = ns;
+            seg_cfg_[3] = bps;
+        } else {
+            throw Error(E_INVALID, "PDFP_SEG must read 0 or segments,long_row_threshold"
+                                   "[,stage_bytes,threads,stages[,blocks_per_segment]]");
+        }
+    }
+    if (seg_mode_ > 0 && precision_ == PDFP_MIXED) {
+        d32_.seg_nseg = seg_mode_;
+        d32_.seg_long = seg_long_;
+        d32_.seg_stage = seg_cfg_[0];
+        d32_.seg_nt = seg_cfg_[1];
+        d32_.seg_stages = seg_cfg_[2];
+        d32_.seg_bps = seg_cfg_[3];
+    }
     // PDFP_TUNING="s,t,l,s,t,l" pins both sides' step kernels of this precision
     // (A' then A: stage bytes, threads per role -- 0: flat engine, whose stage
-    // bytes tell its variant -- and the L2-only gather flag), as pdfp_get_tuning
+    // bytes tell its variant; 32: vec engine, whose "stage bytes" are its nonzeros
+    // per lane, FP32 steps only -- and the L2-only gather flag), as pdfp_get_tuning
     // reports them; the tuner does not run.
     bool pinned = false;
     if (const char* pt = std::getenv("PDFP_TUNING")) {
@@ -818,8 +855,22 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
             for (int f = 0; f < 2; ++f) {
                 StepSide& q = *sides[f][k];
                 const int* c = v + 3 * k;
-                if (c[1] != 0 && c[1] != 128 && c[1] != 256)
-                    throw Error(E_INVALID, "PDFP_TUNING: threads per role must be 0, 128 or 256");
+                if (c[1] != 0 && c[1] != 32 && c[1] != 128 && c[1] != 256)
+                    throw Error(E_INVALID, "PDFP_TUNING: threads per role must be 0, 32, 128 or 256");
+                if (c[1] == 32) {  // the vec engine: FP32 steps; the FP64 steps keep their default
+                    if (c[0] != 1 && c[0] != 2 && c[0] != 4 && c[0] != 8)
+                        throw Error(E_INVALID, "PDFP_TUNING: the vec engine's nonzeros per lane must "
+                                               "be 1, 2, 4 or 8");
+                    if (c[2] < 0 || c[2] > 1)
+                        throw Error(E_INVALID, "PDFP_TUNING: the vec engine's gather policy must be 0 or 1");
+                    if (v[10 + k] != 0)
+                        throw Error(E_INVALID, "PDFP_TUNING: the vec engine has no reducers (0)");
+                    if (f == 1) continue;
+                    q.engine = 2;
+                    q.lane_nnz = c[0];
+                    q.gather_l2 = c[2];
+                    continue;
+                }
                 if (c[1] != 0 && (c[0] < 8192 || c[0] > 49152 || c[0] % 128 != 0))
                     throw Error(E_INVALID, "PDFP_TUNING: tile-engine stage bytes must be a multiple "
                                            "of 128 in [8192, 49152]");
@@ -861,6 +912,11 @@ IterVecs<double>& Projector::vecs<double>() { return v64_; }
 template <typename T, bool MAJOR>
 void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    if constexpr (std::is_same<T, float>::value)
+        if (s.engine == 2) {
+            launch_vec(s.vec, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.grid, stream_);
+            return;
+        }
     if (s.engine == 1)
         launch_flat(s.tiling.dev, PrimalOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
@@ -872,6 +928,18 @@ void Projector::launch_primal(const StepSide& s, int k, bool overlap) {
 template <typename T, bool MAJOR>
 void Projector::launch_dual(const StepSide& s, int k, bool overlap) {
     const int mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
+    if constexpr (std::is_same<T, float>::value) {
+        if (s.engine == 2) {
+            launch_vec(s.vec, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.grid, stream_);
+            return;
+        }
+        if (s.seg_nseg > 0) {  // the long rows first; the tile launch then follows no step launch
+            launch_seg(s.segt.dev, s.segd, s.seg_nt, s.seg_bps,
+                       DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2},
+                       stream_);
+            overlap = false;
+        }
+    }
     if (s.engine == 1)
         launch_flat(s.tiling.dev, DualOp<T, MAJOR, kFlatThreads>{vecs<T>(), st_, M_.row_off, M_.n_eq, k, mode, err_, s.gather_l2}, s.qpt, s.grid, stream_);
     else if (s.nt == 256)
@@ -894,6 +962,22 @@ static int step_grid(const SideDev& d, int nt, int sms, bool async, bool half_re
 
 void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     const int e = f32 ? 4 : 8;
+    if (s.engine != 0) s.seg_nseg = 0;  // segmented long rows: tile engine only
+    if (s.engine == 2) {
+        if (!f32) throw Error(E_INVALID, "internal: the vec engine runs the FP32 steps only");
+        s.vec = M_.make_vec(ar_, primal, s.lane_nnz);
+        s.stage_bytes = s.lane_nnz;
+        s.nt = 32;
+        s.half_red = false;
+        if (s.gather_l2 == 2) s.gather_l2 = 1;
+        // both the MAJOR and the minor kernel: the grid is the smaller of the two
+        const int g0 = primal ? vec_grid<PrimalOp<float, false, kFlatThreads>>(s.vec, num_sms_)
+                              : vec_grid<DualOp<float, false, kFlatThreads>>(s.vec, num_sms_);
+        const int g1 = primal ? vec_grid<PrimalOp<float, true, kFlatThreads>>(s.vec, num_sms_)
+                              : vec_grid<DualOp<float, true, kFlatThreads>>(s.vec, num_sms_);
+        s.grid = std::min(g0, g1);
+        return;
+    }
     if (s.engine == 1) {
         const int cap = s.qpt * 4 * kFlatThreads;
         s.stage_bytes = flat_stage_bytes(e, cap);
@@ -911,7 +995,25 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
         return;
     }
     StageGeom g{e, e, e, primal ? 8 : 3, 1, s.stage_bytes, 2048};
-    s.tiling = M_.make_tiling(ar_, primal, g);
+    std::vector<uint8_t> is_long;
+    const std::vector<uint8_t>* skip = nullptr;
+    if (s.seg_nseg > 0) {
+        if (primal || !f32) throw Error(E_INVALID, "internal: segmented long rows are an FP32 A-side form");
+        const StageGeom gs{4, 4, 4, 0, 1, s.seg_stage, 2048};
+        const DualOp<float, false, kFlatThreads> dop{v32_, st_, M_.row_off, M_.n_eq, 0, MODE_FP32, err_, 0};
+        bool ok = M_.make_seg(ar_, s.seg_nseg, s.seg_long, gs, s.segd, s.segt, is_long);
+        if (ok) {
+            s.segt.dev.stages = s.seg_stages;
+            s.segt.dev.evict_first = evict_first_ ? 1 : 0;
+            ok = s.seg_nt == 256 ? seg_attr<256>(s.segt.dev, s.segd, dop, max_smem_block_)
+                                 : seg_attr<128>(s.segt.dev, s.segd, dop, max_smem_block_);
+        }
+        if (ok)
+            skip = &is_long;
+        else
+            s.seg_nseg = 0;  // no row qualifies, or a segment does not fit a block
+    }
+    s.tiling = M_.make_tiling(ar_, primal, g, skip);
     s.tiling.dev.stages = s.stages;
     s.tiling.dev.evict_first = evict_first_ ? 1 : 0;
     const bool async = s.gather_l2 == 2;
@@ -944,9 +1046,10 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
 }
 
 // The autotuner: times the minor step kernel of each side for every candidate
-// (shared-memory stage size x threads per role x gather cache policy) on this
-// handle's matrix, twice, and keeps the fastest.  Runs at creation on the
-// all-zero state, which it resets afterwards.
+// (engine, shared-memory stage size x threads per role x gather cache policy, and
+// for the FP32 A side a few segmentations of its long rows) on this handle's
+// matrix, each launch right after one of the other side's step, twice, and keeps
+// the fastest.  Runs at creation on the all-zero state, which it resets afterwards.
 void Projector::autotune(bool f32) {
     struct Cand {
         int engine, stage, nt, l2, qpt, stages;
@@ -978,11 +1081,54 @@ void Projector::autotune(bool f32) {
         {0, 24 * 1024, 256, 0, 0, 2, 0, 1}, {0, 32 * 1024, 256, 1, 0, 2, 0, 1},
         // gather policy 2: per-thread async copies into the stage (FP32 steps)
         {0, 12 * 1024, 128, 2, 0, 3}, {0, 20 * 1024, 128, 2, 0, 3}, {0, 24 * 1024, 128, 2, 0, 3},
-        {0, 32 * 1024, 256, 2, 0, 4}};
+        {0, 32 * 1024, 256, 2, 0, 4},
+        // the vec engine (FP32 steps): nonzeros per lane x gather cache policy
+        {2, 1, 32, 0, 0, 4}, {2, 1, 32, 1, 0, 4}, {2, 2, 32, 0, 0, 4}, {2, 2, 32, 1, 0, 4},
+        {2, 4, 32, 0, 0, 4}, {2, 4, 32, 1, 0, 4}, {2, 8, 32, 0, 0, 4}, {2, 8, 32, 1, 0, 4}};
     constexpr int NC = sizeof(cands) / sizeof(cands[0]);
     cudaEvent_t e0, e1;
     PDFP_CK(cudaEventCreate(&e0));
     PDFP_CK(cudaEventCreate(&e1));
+    // Mean time of one minor step launch of a side (1e30 if it cannot launch), each
+    // launch timed right after one of the other side's step (`partner`), as a PDHG
+    // iteration runs them: the partner has just streamed its matrix through L2, so
+    // the candidate finds the cache as it will in the solves (timed back to back
+    // against itself, a candidate would find its own per-row vectors still in L2).
+    auto run_side = [&](const StepSide& q, bool pr, int k) {
+        if (pr) {
+            if (f32) launch_primal<float, false>(q, k); else launch_primal<double, false>(q, k);
+        } else {
+            if (f32) launch_dual<float, false>(q, k); else launch_dual<double, false>(q, k);
+        }
+    };
+    auto time_side = [&](const StepSide& s, bool primal, const StepSide& partner) -> float {
+        run_side(s, primal, 2);
+        run_side(s, primal, 3);
+        if (cudaGetLastError() != cudaSuccess) return 1e30f;  // candidate cannot launch
+        const int reps = 8;
+        float total = 0.f;
+        for (int r = 0; r < reps; ++r) {
+            run_side(partner, !primal, 4 + r);
+            PDFP_CK(cudaEventRecord(e0, stream_));
+            run_side(s, primal, 4 + r);
+            PDFP_CK(cudaEventRecord(e1, stream_));
+            PDFP_CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PDFP_CK(cudaEventElapsedTime(&ms, e0, e1));
+            total += ms;
+        }
+        PDFP_CK(cudaGetLastError());
+        return total / reps;
+    };
+    // the A side's partner while A' is tuned: a tile configuration that does well on
+    // large matrices (then A is tuned against the chosen A' side)
+    StepSide dual0;
+    dual0.stage_bytes = 24 * 1024;
+    dual0.nt = 128;
+    dual0.gather_l2 = 1;
+    dual0.stages = 2;
+    dual0.max_blocks = 3;
+    prepare_side(dual0, false, f32);
     tune_table_.clear();
     for (int side = 0; side < 2; ++side) {
         const bool primal = side == 0;
@@ -998,6 +1144,10 @@ void Projector::autotune(bool f32) {
             sides[i].gather_l2 = cands[i].l2;
             sides[i].max_blocks = cands[i].max_blocks;
             sides[i].half_red = cands[i].half_red != 0;
+            if (cands[i].engine == 2) {
+                if (!f32) continue;  // FP32 steps only
+                sides[i].lane_nnz = cands[i].stage;
+            }
             prepare_side(sides[i], primal, f32);
             if (sides[i].grid <= 0) empty_side = true;
         }
@@ -1009,37 +1159,56 @@ void Projector::autotune(bool f32) {
         for (int sweep = 0; sweep < 2; ++sweep) {
             for (int i = 0; i < NC; ++i) {
                 if (cands[i].l2 == 2 && !f32) continue;  // FP64 steps have no async policy
-                const StepSide& s = sides[i];
-                auto run = [&](int k) {
-                    if (primal) {
-                        if (f32) launch_primal<float, false>(s, k); else launch_primal<double, false>(s, k);
-                    } else {
-                        if (f32) launch_dual<float, false>(s, k); else launch_dual<double, false>(s, k);
-                    }
-                };
-                run(2);
-                run(3);
-                if (cudaGetLastError() != cudaSuccess) continue;  // candidate cannot launch
-                PDFP_CK(cudaEventRecord(e0, stream_));
-                const int reps = 8;
-                for (int r = 0; r < reps; ++r) run(4 + r);
-                PDFP_CK(cudaEventRecord(e1, stream_));
-                PDFP_CK(cudaEventSynchronize(e1));
-                PDFP_CK(cudaGetLastError());
-                float ms = 0.f;
-                PDFP_CK(cudaEventElapsedTime(&ms, e0, e1));
-                best_ms[i] = std::min(best_ms[i], ms / reps);
+                if (cands[i].engine == 2 && !f32) continue;
+                best_ms[i] = std::min(best_ms[i], time_side(sides[i], primal,
+                                                            primal ? dual0 : (f32 ? p32_ : p64_)));
             }
         }
         int bi = 0;
         for (int i = 0; i < NC; ++i) {
             tune_table_.push_back(TuneRow{side, sides[i].stage_bytes, cands[i].nt, cands[i].l2, cands[i].stages,
                                           cands[i].max_blocks,
-                                          sides[i].half_red ? cands[i].nt / 2 : cands[i].nt, best_ms[i]});
+                                          cands[i].engine == 2 ? 0
+                                          : sides[i].half_red ? cands[i].nt / 2 : cands[i].nt,
+                                          best_ms[i]});
             if (best_ms[i] < best_ms[bi]) bi = i;
         }
         dst = sides[bi];
         dst.tuned_ms = best_ms[bi];
+        // the A side of the FP32 steps with its long rows by column segment, on the
+        // chosen tile configuration for the rest
+        if (f32 && !primal && dst.engine == 0 && seg_mode_ != 0) {
+            struct SegCand {
+                int nseg, lmin, stage, nt, stages, bps;
+            };
+            std::vector<SegCand> sc;
+            if (seg_mode_ > 0)
+                sc.push_back({seg_mode_, seg_long_, seg_cfg_[0], seg_cfg_[1], seg_cfg_[2], seg_cfg_[3]});
+            else if (M_.L.NNZ >= (int64_t(1) << 22))
+                sc = {{num_sms_, 512, 24 * 1024, 256, 3, 1},     {num_sms_, 1024, 16 * 1024, 128, 3, 2},
+                      {num_sms_, 512, 16 * 1024, 128, 3, 2},     {2 * num_sms_, 1024, 16 * 1024, 128, 3, 1},
+                      {2 * num_sms_, 512, 12 * 1024, 128, 2, 2}, {num_sms_, 512, 32 * 1024, 256, 3, 1}};
+            const StepSide keep = dst;
+            for (const SegCand& q : sc) {
+                StepSide c = keep;
+                c.seg_nseg = q.nseg;
+                c.seg_long = q.lmin;
+                c.seg_stage = q.stage;
+                c.seg_nt = q.nt;
+                c.seg_stages = q.stages;
+                c.seg_bps = q.bps;
+                prepare_side(c, false, true);
+                if (c.seg_nseg == 0) continue;  // not applicable to this matrix
+                float ms = 1e30f;
+                for (int sweep = 0; sweep < 2; ++sweep) ms = std::min(ms, time_side(c, false, p32_));
+                tune_table_.push_back(TuneRow{2, q.nseg, q.lmin, c.gather_l2, q.stages, q.stage,
+                                              q.nt, ms});
+                if (seg_mode_ > 0 || ms < dst.tuned_ms) {
+                    dst = c;
+                    dst.tuned_ms = ms;
+                }
+            }
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1080,12 +1249,18 @@ void Projector::tuning_blocks(int32_t* out) const {
     out[1] = (f32 ? d32_ : d64_).max_blocks;
 }
 
+void Projector::tuning_seg(int32_t* out) const {
+    const StepSide& d = precision_ == PDFP_MIXED ? d32_ : d64_;
+    out[0] = d.seg_nseg;
+    out[1] = d.seg_nseg > 0 ? d.seg_long : 0;
+}
+
 void Projector::tuning_reducers(int32_t* out) const {
     const bool f32 = precision_ == PDFP_MIXED;
     const StepSide& p = f32 ? p32_ : p64_;
     const StepSide& d = f32 ? d32_ : d64_;
-    out[0] = p.engine == 1 ? 0 : (p.half_red ? p.nt / 2 : p.nt);
-    out[1] = d.engine == 1 ? 0 : (d.half_red ? d.nt / 2 : d.nt);
+    out[0] = p.engine != 0 ? 0 : (p.half_red ? p.nt / 2 : p.nt);
+    out[1] = d.engine != 0 ? 0 : (d.half_red ? d.nt / 2 : d.nt);
 }
 
 void Projector::tuning(int32_t* out) const {
@@ -1094,10 +1269,10 @@ void Projector::tuning(int32_t* out) const {
     const StepSide& d = f32 ? d32_ : d64_;
     out[0] = p.stage_bytes;
     out[1] = p.nt;
-    out[2] = p.tiling.dev.n_tiles;
+    out[2] = p.engine == 2 ? p.vec.n_items : p.tiling.dev.n_tiles;
     out[3] = d.stage_bytes;
     out[4] = d.nt;
-    out[5] = d.tiling.dev.n_tiles;
+    out[5] = d.engine == 2 ? d.vec.n_items : d.tiling.dev.n_tiles;
     out[6] = p.gather_l2;
     out[7] = d.gather_l2;
 }

@@ -60,17 +60,33 @@ class Projector {
     void tuning_stages(int32_t* out) const;
     void tuning_blocks(int32_t* out) const;
     void tuning_reducers(int32_t* out) const;
+    // The A-side step of the FP32 steps with its long rows by column segment:
+    // {segments, long-row threshold}, {0, 0} when it has none.
+    void tuning_seg(int32_t* out) const;
     // Every autotuner measurement: ms[i] and cfg[7i..7i+6] = {side (0: A', 1: A),
     // stage bytes, gatherer threads, gather policy, stages, blocks per SM cap,
-    // reducer threads}; returns the count.
+    // reducer threads}; side 2: the A side with its long rows by column segment,
+    // {2, segments, long-row threshold, gather policy of the other rows, the
+    // partials' stages, stage bytes and threads per role}; returns the count.
     int tuning_table(float* ms, int32_t* cfg, int cap) const;
     void set_kernel_timing(bool on);
 
   private:
     // One side of the PDHG step: its tile geometry, block size and tiling.
     struct StepSide {
-        int engine = 0;  // 0: tile engine (tile_spmv.cuh), 1: flat engine (flat_spmv.cuh)
+        int engine = 0;  // 0: tile engine (tile_spmv.cuh), 1: flat engine (flat_spmv.cuh),
+                         // 2: vec engine (vec_spmv.cuh; FP32 steps)
         int qpt = 2;     // flat engine: quads (4 nonzeros) per thread and tile, 1 or 2
+        int lane_nnz = 4;  // vec engine: target nonzeros per lane of a row
+        VecDev vec{};      // vec engine: its items
+        // A side, FP32, tile engine: rows of at least seg_long nonzeros regrouped by
+        // column segment (seg_spmv.cuh; seg_nseg segments, 0: off); the tiling then
+        // covers the other rows
+        int seg_nseg = 0, seg_long = 0;
+        int seg_stage = 16 * 1024, seg_nt = 128, seg_stages = 3;  // the partials' tile engine
+        int seg_bps = 1;  // its blocks per segment
+        SegDev segd{};
+        DeviceMatrix::Tiling segt;  // tiling of the (segment, long row) pairs
         int stages = 4;  // tile engine: shared-memory stages per block, 2..4
         int max_blocks = 0;  // tile engine: resident blocks per SM cap (0: as many as fit)
         int carveout = -1;   // preferred shared-memory share of L1 for that cap (percent)
@@ -83,7 +99,7 @@ class Projector {
         float tuned_ms = 0.f;
     };
     struct TuneRow {
-        int side, stage, nt, l2;  // nt = 0: the flat engine
+        int side, stage, nt, l2;  // nt = 0: the flat engine; nt = 32: the vec engine (stage = lane_nnz)
         int stages;
         int max_blocks;
         int reducers;
@@ -127,6 +143,11 @@ class Projector {
     int K_ = 0;
     int num_sms_ = 148;
     int max_smem_sm_ = 233472;  // unified L1 / shared memory usable as shared, per SM
+    int max_smem_block_ = 232448;  // shared memory one block may opt in to
+    int seg_mode_ = -1;  // segmented long rows: -1 autotuned, 0 off, > 0 that many segments
+    int seg_long_ = 0;   // with seg_mode_ > 0: the long-row threshold
+    int seg_cfg_[4] = {16 * 1024, 128, 3, 1};  // and the partials' stage bytes, threads, stages,
+                                               // blocks per segment
     cudaStream_t stream_ = nullptr;
     DeviceArena ar_;
     DeviceMatrix M_;

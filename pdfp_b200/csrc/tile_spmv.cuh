@@ -92,6 +92,16 @@ template <class Op>
 constexpr bool kAsyncEligible = HasGatherSrc<Op>::value && sizeof(typename Op::MT) == 4 &&
                                 sizeof(typename Op::AT) == 4 && Op::NV == 1;
 
+// Ops that gather from a block-private copy in shared memory (after the stages and
+// row sums; extra_smem() bytes) fill it in prologue(), run by the gatherers, which
+// then meet at a named barrier before their first gather.
+template <class Op, class = void>
+struct HasPrologue : std::false_type {};
+template <class Op>
+struct HasPrologue<Op, std::void_t<decltype(std::declval<const Op&>().prologue(0, 0))>>
+    : std::true_type {};
+constexpr int kGatherBar = 3;  // named barrier id of the gatherer threads
+
 template <class Op>
 struct TileKernelSmem {
     static constexpr int NP = Op::NP > 0 ? Op::NP : 1;
@@ -219,6 +229,10 @@ __global__ void __launch_bounds__(Op::NT + NRED + 32) tile_spmv_kernel(const Sid
         // ---- gatherers: products of each chunk, in place over its values ----
         const int g = threadIdx.x;
         griddep_wait();  // the gathered vector comes from the previous grid
+        if constexpr (HasPrologue<Op>::value) {
+            op.prologue(g, NT);
+            named_sync(kGatherBar, NT);
+        }
         for (uint32_t u = 0;; ++u) {
             const int st = u % NS;
             // Each gatherer waits and arrives on its own: with no barrier among them a

@@ -23,6 +23,7 @@ static int check_tiling(const HostCsr& csr, const std::vector<int32_t>& off, con
         for (int32_t tt = t.inst_tile0[p]; tt < t.inst_tile0[p + 1]; ++tt) {
             if (t.tile_inst[tt] != p) return 12;
             if (t.tile_row[tt] != r) return 13;
+            if (t.tile_row_end[tt] != t.tile_row[tt + 1]) return 27;  // no row left out
             const int32_t r0 = t.tile_row[tt], r1 = t.tile_row[tt + 1];
             if (r1 <= r0) return 14;
             if (r0 < off[p] || r1 > off[p + 1]) return 15;  // a tile never crosses an instance
@@ -51,6 +52,152 @@ static int check_tiling(const HostCsr& csr, const std::vector<int32_t>& off, con
         r = off[p + 1];
     }
     *n_tiles += static_cast<int64_t>(t.tile_inst.size());
+    return 0;
+}
+
+// Vec-engine items (build_vec_items): every row once, in a multi-row item of its
+// instance or as pieces that cover its nonzeros in order; lanes and sizes in range.
+static int check_vec(const HostCsr& csr, const std::vector<int32_t>& off, int lane_nnz) {
+    std::vector<VecItem> items;
+    const int32_t slots = build_vec_items(csr, off, lane_nnz, items);
+    const int K = static_cast<int>(off.size()) - 1;
+    std::vector<int> seen(csr.rows, 0);
+    std::vector<int32_t> next_k(csr.rows, -1);
+    std::vector<int> slot_used(slots > 0 ? slots : 1, 0);
+    bool pieces_done = false;
+    int last_lg = 6;
+    for (const VecItem& it : items) {
+        if (it.inst < 0 || it.inst >= K) return 1;
+        if (it.lg < 0) {
+            if (pieces_done) return 2;  // pieces come first
+            const int32_t r = it.r0;
+            if (r < off[it.inst] || r >= off[it.inst + 1]) return 3;
+            const int32_t len = csr.rp[r + 1] - csr.rp[r];
+            if (len <= kVecPiece || it.np != (len + kVecPiece - 1) / kVecPiece) return 4;
+            if (next_k[r] < 0) next_k[r] = csr.rp[r];
+            if (it.k0 != next_k[r] || it.k1 <= it.k0 || it.k1 - it.k0 > kVecPiece) return 5;
+            if (it.slot != it.r1 + (it.k0 - csr.rp[r]) / kVecPiece || it.slot >= slots) return 6;
+            slot_used[it.slot]++;
+            next_k[r] = it.k1;
+            if (it.k1 == csr.rp[r + 1]) seen[r]++;
+            continue;
+        }
+        pieces_done = true;
+        if (it.lg > 5 || it.lg > last_lg) return 7;  // by decreasing lanes per row
+        last_lg = it.lg;
+        if (it.r1 <= it.r0 || it.r0 < off[it.inst] || it.r1 > off[it.inst + 1]) return 8;
+        for (int32_t r = it.r0; r < it.r1; ++r) {
+            if (csr.rp[r + 1] - csr.rp[r] > kVecPiece) return 9;
+            seen[r]++;
+        }
+    }
+    for (int32_t r = 0; r < csr.rows; ++r)
+        if (seen[r] != 1) return 10;
+    for (int32_t q = 0; q < slots; ++q)
+        if (slot_used[q] != 1) return 11;
+    return 0;
+}
+
+// Segmented long rows (build_seg), the interleaved tiling of their pairs and the
+// tiling of the other rows: the long rows are exactly those of at least long_min
+// nonzeros, each pair holds the row's entries of its segment in storage order, block
+// s of an nseg grid walks exactly segment s's tiles, and the tiling with the long
+// rows left out covers every other row once.
+static int check_seg(const HostCsr& A, const std::vector<int32_t>& off, int nseg, int long_min,
+                     int stage_bytes, int64_t* n_long_out) {
+    HostSeg h;
+    const bool ok = build_seg(A, off, nseg, long_min, h);
+    const int K = static_cast<int>(off.size()) - 1;
+    const int64_t seg_len = A.cols > 0 ? (((A.cols + nseg - 1) / nseg + 3) & ~int64_t(3)) : 0;
+    int64_t n_want = 0;
+    for (int32_t r = 0; r < A.rows; ++r) n_want += A.rp[r + 1] - A.rp[r] >= long_min;
+    if (!ok) return (n_want == 0 || seg_len > 65536 || A.cols == 0) && h.long_row.empty() ? 0 : 1;
+    const int64_t nl = static_cast<int64_t>(h.long_row.size());
+    if (nl != n_want || h.seg_len != seg_len || (int64_t)h.is_long.size() != A.rows) return 2;
+    for (int32_t r = 0; r < A.rows; ++r)
+        if (h.is_long[r] != (A.rp[r + 1] - A.rp[r] >= long_min)) return 3;
+    for (int64_t q = 0; q < nl; ++q) {
+        const int32_t r = h.long_row[q];
+        if (!h.is_long[r] || (q > 0 && r <= h.long_row[q - 1])) return 4;
+        const int p = h.long_inst[q];
+        if (p < 0 || p >= K || r < off[p] || r >= off[p + 1]) return 5;
+    }
+    const HostCsr& P = h.pairs;
+    if (P.rows != nseg * nl || (int64_t)P.rp.size() != P.rows + 1 || P.rp[0] != 0) return 6;
+    for (size_t i = 1; i < P.rp.size(); ++i)
+        if (P.rp[i] < P.rp[i - 1]) return 6;
+    if (P.rp.back() != (int32_t)P.ci.size() || P.ci.size() != P.v.size()) return 7;
+    // each pair: the long row's entries of its segment, in storage order
+    int64_t total = 0;
+    for (int64_t q = 0; q < nl; ++q) {
+        const int32_t r = h.long_row[q];
+        for (int s = 0; s < nseg; ++s) {
+            int32_t e = P.rp[s * nl + q];
+            const int32_t e1 = P.rp[s * nl + q + 1];
+            total += e1 - e;
+            for (int32_t k = A.rp[r]; k < A.rp[r + 1]; ++k) {
+                if (A.ci[k] / seg_len != s) continue;
+                if (e >= e1) return 9;
+                if (P.ci[e] + s * seg_len != A.ci[k] || P.ci[e] < 0 || P.ci[e] >= seg_len ||
+                    P.v[e] != A.v[k])
+                    return 10;
+                ++e;
+            }
+            if (e != e1) return 11;
+        }
+    }
+    if (total != P.rp.back()) return 11;
+    // tiles by segment, interleaved
+    std::vector<int32_t> soff(nseg + 1);
+    for (int s = 0; s <= nseg; ++s) soff[s] = static_cast<int32_t>(s * nl);
+    const StageGeom gs{4, 4, 4, 0, 1, stage_bytes, 2048};
+    HostTiling by, t;
+    build_tiling(P, soff, gs, by);
+    interleave_tiles(by, nseg, t);
+    if (t.tile_chunk.size() != t.tile_inst.size() + 1 || t.tile_row_end.size() != t.tile_inst.size() ||
+        t.tile_inst.size() % nseg != 0)
+        return 12;
+    std::vector<int> pair_cover(P.rows, 0);
+    for (int b = 0; b < nseg; ++b)
+        for (size_t tt = b; tt < t.tile_inst.size(); tt += nseg) {
+            const int32_t p = t.tile_inst[tt];
+            if (p == -1) {
+                if (t.tile_chunk[tt + 1] != t.tile_chunk[tt]) return 13;
+                continue;
+            }
+            if (p != b) return 14;  // block b sees only its own segment
+            const int32_t r0 = t.tile_row[tt], r1 = t.tile_row_end[tt];
+            if (r1 <= r0 || r0 < soff[b] || r1 > soff[b + 1]) return 15;
+            int64_t k = P.rp[r0];
+            for (int32_t c = t.tile_chunk[tt]; c < t.tile_chunk[tt + 1]; ++c) {
+                if (t.chunk_tile[c] != (int32_t)tt || t.chunk_k0[c] != k) return 16;
+                k = t.chunk_k1[c];
+            }
+            if (k != P.rp[r1]) return 17;
+            for (int32_t r = r0; r < r1; ++r) pair_cover[r]++;
+        }
+    for (int32_t r = 0; r < P.rows; ++r)
+        if (pair_cover[r] != 1) return 18;
+    // the tiling of the other rows
+    const StageGeom g{4, 4, 4, 3, 1, 16 * 1024, 2048};
+    HostTiling o;
+    build_tiling(A, off, g, o, &h.is_long);
+    std::vector<int> cover(A.rows, 0);
+    for (size_t tt = 0; tt < o.tile_inst.size(); ++tt) {
+        const int32_t r0 = o.tile_row[tt], r1 = o.tile_row_end[tt];
+        const int p = o.tile_inst[tt];
+        if (r1 <= r0 || r0 < off[p] || r1 > off[p + 1]) return 19;
+        int64_t k = A.rp[r0];
+        for (int32_t c = o.tile_chunk[tt]; c < o.tile_chunk[tt + 1]; ++c) {
+            if (o.chunk_k0[c] != k) return 20;
+            k = o.chunk_k1[c];
+        }
+        if (k != A.rp[r1]) return 21;
+        for (int32_t r = r0; r < r1; ++r) cover[r]++;
+    }
+    for (int32_t r = 0; r < A.rows; ++r)
+        if (cover[r] != (h.is_long[r] ? 0 : 1)) return 22;
+    *n_long_out += nl;
     return 0;
 }
 
@@ -118,5 +265,20 @@ extern "C" int layout_check(int K, const int32_t* ms, const int32_t* ns, const i
             rc = check_tiling(L.A, L.row_off, g, &stats[0], &stats[1], cap);
             if (rc) return 300 + rc;
         }
+    // the vec engine's items
+    for (int lane : {1, 2, 4, 8}) {
+        int rc = check_vec(L.At, L.col_off, lane);
+        if (rc) return 400 + rc;
+        rc = check_vec(L.A, L.row_off, lane);
+        if (rc) return 500 + rc;
+    }
+    // segmented long rows: small stages, so that pairs span several tiles and long
+    // pairs several chunks
+    stats[2] = 0;
+    const int segs[][3] = {{1, 1, 8192}, {3, 2, 8192}, {16, 4, 8192}, {64, 64, 16384}, {7, 16, 8192}};
+    for (const auto& c : segs) {
+        int rc = check_seg(L.A, L.row_off, c[0], c[1], c[2], &stats[2]);
+        if (rc) return 600 + rc;
+    }
     return 0;
 }

@@ -183,3 +183,21 @@ def test_set_polish_rejects_bad_arguments():
     assert L.lib().pdfp_set_polish(g._h, 10, 0.0) == L.E_INVALID
     assert L.lib().pdfp_set_polish(g._h, 10, 1.0) == L.E_INVALID
     assert L.lib().pdfp_set_polish(None, 10, 1e-6) == L.E_INVALID
+
+
+@pytest.mark.parametrize("name", ["zipf-4k", "zipf-100k"])
+def test_vec_engine_matches_oracle(oracle, name, monkeypatch):
+    """The same bars with the FP32 steps on the vec engine (vec_spmv.cuh): tight
+    tolerance through the FP64 polish, and the benchmark tolerance in FP32."""
+    monkeypatch.setenv("PDFP_STEP_ENGINE", "vec")
+    test_mixed_tight_matches_oracle(oracle, name, 1e-8)
+    test_mixed_at_bench_tolerance_stays_fp32(oracle, name)
+
+
+@pytest.mark.parametrize("name,seg", [("zipf-4k", "64,256"), ("zipf-100k", "148,512")])
+def test_segmented_long_rows_match_oracle(oracle, name, seg, monkeypatch):
+    """The same bars with the A side's long rows by column segment (seg_spmv.cuh)."""
+    monkeypatch.setenv("PDFP_STEP_ENGINE", "tile")
+    monkeypatch.setenv("PDFP_SEG", seg)
+    test_mixed_tight_matches_oracle(oracle, name, 1e-8)
+    test_mixed_at_bench_tolerance_stays_fp32(oracle, name)

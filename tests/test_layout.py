@@ -51,8 +51,9 @@ def run(lib, mats, eqs, stage_bytes=40 * 1024):
         cis[p] = ci.ctypes.data_as(C.POINTER(C.c_int32))
         vs[p] = v.ctypes.data_as(C.POINTER(C.c_double))
         es[p] = ee.ctypes.data_as(C.POINTER(C.c_uint8))
-    stats = (C.c_int64 * 2)()
+    stats = (C.c_int64 * 3)()
     rc = lib.layout_check(K, ms, ns, rps, cis, vs, es, stage_bytes, stats)
+    run.n_seg_long = stats[2]  # long rows taken by the segmented form, summed over its cases
     return rc, stats[0], stats[1]
 
 
@@ -76,6 +77,7 @@ def test_layout_long_rows_split_into_chunks(checker):
     A = rand_csr(rng, 50, 40000, 0.0005, long_rows=3, long_len=30000)
     rc, tiles, n_long = run(checker, [A], [np.zeros(50, bool)], stage_bytes=16 * 1024)
     assert rc == 0 and n_long > 0
+    assert run.n_seg_long > 0  # the segmented form took long rows
 
 
 def test_layout_batch_with_empty_rows_cols_and_instances(checker):
