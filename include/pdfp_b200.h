@@ -269,11 +269,12 @@ PDFP_API int pdfp_get_tuning_reducers(const pdfp_handle* h, int32_t* out);
  * handle runs it without.  The rows with at least that many nonzeros are summed
  * by one block per column segment, gathering from that segment of x_bar held in
  * shared memory, and finished one warp per row (FP64 sum of the segments'
- * partials in segment order); the other rows stay on the tile engine.  The
- * autotuner tries a few segmentations on handles of at least 2^22 nonzeros
- * and keeps one only if it beats the tile engine's A-side step.  PDFP_SEG=0
- * switches this off; PDFP_SEG="n,l[,s,t,k]" fixes n segments and threshold l
- * (and the partials pass's stage bytes, threads per role and stages). */
+ * partials in segment order); the other rows stay on the tile engine.  Off
+ * by default.  PDFP_SEG=tune lets the autotuner try a few segmentations on
+ * handles of at least 2^22 nonzeros and keep one only if it beats the tile
+ * engine's A-side step; PDFP_SEG="n,l[,s,t,k[,b]]" fixes n segments and
+ * threshold l (and the partials pass's stage bytes, threads per role, stages
+ * and blocks per segment); PDFP_SEG=0: off. */
 PDFP_API int pdfp_get_tuning_seg(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
  * launch time, cfg[7i..7i+6] = {side (0: A', 1: A), stage bytes, gatherer

@@ -801,15 +801,19 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
             q->qpt = qpt;
         }
     }
-    // PDFP_SEG=0 keeps the A side's long rows on the step engine; PDFP_SEG="n,l"
-    // regroups the rows of at least l nonzeros into n column segments (seg_spmv.cuh)
-    // whenever the FP32 A side runs on the tile engine; unset, the autotuner tries
-    // a few such forms against the plain tile engine.
+    // The A side's long rows by column segment (seg_spmv.cuh), FP32 steps on the tile
+    // engine: PDFP_SEG="n,l" regroups the rows of at least l nonzeros into n column
+    // segments; PDFP_SEG=tune lets the autotuner try a few such forms against the
+    // plain tile engine; unset or 0, the long rows stay on the step engine (on the
+    // zipf-lp matrices measured so far the form was slower, and building its
+    // candidates costs about a second per large handle).
     // Optional after them: the partials' stage bytes, threads per role and stages.
     if (const char* sg = std::getenv("PDFP_SEG")) {
         int n = 0, l = 0, sb = d32_.seg_stage, nt = d32_.seg_nt, ns = d32_.seg_stages, bps = 1;
         const int got = std::sscanf(sg, "%d,%d,%d,%d,%d,%d", &n, &l, &sb, &nt, &ns, &bps);
-        if (got == 1 && n == 0) {
+        if (std::strcmp(sg, "tune") == 0) {
+            seg_mode_ = -1;
+        } else if (got == 1 && n == 0) {
             seg_mode_ = 0;
         } else if ((got == 2 || got == 5 || got == 6) && n > 0 && n <= 65536 && l > 0 &&
                    sb >= 8192 && sb <= 49152 && sb % 128 == 0 && (nt == 128 || nt == 256) &&
@@ -821,7 +825,7 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
             seg_cfg_[2] = ns;
             seg_cfg_[3] = bps;
         } else {
-            throw Error(E_INVALID, "PDFP_SEG must read 0 or segments,long_row_threshold"
+            throw Error(E_INVALID, "PDFP_SEG must read 0, tune or segments,long_row_threshold"
                                    "[,stage_bytes,threads,stages[,blocks_per_segment]]");
         }
     }

@@ -144,7 +144,7 @@ class Projector {
     int num_sms_ = 148;
     int max_smem_sm_ = 233472;  // unified L1 / shared memory usable as shared, per SM
     int max_smem_block_ = 232448;  // shared memory one block may opt in to
-    int seg_mode_ = -1;  // segmented long rows: -1 autotuned, 0 off, > 0 that many segments
+    int seg_mode_ = 0;  // segmented long rows: -1 autotuned, 0 off, > 0 that many segments
     int seg_long_ = 0;   // with seg_mode_ > 0: the long-row threshold
     int seg_cfg_[4] = {16 * 1024, 128, 3, 1};  // and the partials' stage bytes, threads, stages,
                                                // blocks per segment

@@ -204,9 +204,10 @@ class PDFPState:
         return out[:self.n]
 
     def tuning(self):
-        """The step kernels' configuration (pdfp_get_tuning): A' stage bytes, threads,
-        tiles, A stage bytes, threads, tiles, A' gather policy, A gather policy (3: the
-        segmented engine)."""
+        """The step kernels' configuration (pdfp_get_tuning): A' stage bytes, threads
+        per role (0: flat engine, 32: vec engine, whose stage bytes are its nonzeros per
+        lane), tiles (vec engine: work items), the same three for A, then the A' and A
+        gather policies."""
         out = (C.c_int32 * 8)()
         L.check(L.lib().pdfp_get_tuning(self._h, out))
         return list(out)

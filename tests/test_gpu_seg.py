@@ -127,3 +127,16 @@ def test_seg_bad_env(zipf, monkeypatch, bad):
     monkeypatch.setenv("PDFP_SEG", bad)
     with pytest.raises(Exception, match="PDFP_SEG"):
         solve(zipf)
+
+
+def test_seg_off_by_default_and_tune_accepted(zipf, monkeypatch):
+    """Unset, the long rows stay on the step engine; PDFP_SEG=tune hands the choice
+    to the autotuner (which tries segmentations on handles of at least 2^22 nonzeros
+    only, so this smaller handle keeps the plain form)."""
+    monkeypatch.delenv("PDFP_STEP_ENGINE", raising=False)
+    monkeypatch.delenv("PDFP_SEG", raising=False)
+    s, st, _ = solve(zipf)
+    assert st == "OPTIMAL" and seg_of(s) == [0, 0]
+    monkeypatch.setenv("PDFP_SEG", "tune")
+    s, st, _ = solve(zipf)
+    assert st == "OPTIMAL" and seg_of(s) == [0, 0]
