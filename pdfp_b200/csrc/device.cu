@@ -153,6 +153,25 @@ void DeviceMatrix::upload(DeviceArena& ar, bool want_f32) {
     }
 }
 
+__global__ void recip_kernel(const double* __restrict__ s, double* __restrict__ d, int64_t n) {
+    for (int64_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += int64_t(gridDim.x) * 256)
+        d[i] = __ddiv_rn(1.0, s[i]);
+}
+
+void cast_f64_to_f32(const double* src, float* dst, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 4096));
+    f64_to_f32_kernel<<<blocks, 256, 0, s>>>(src, dst, n);
+    PDFP_CK(cudaGetLastError());
+}
+
+void reciprocal(const double* src, double* dst, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 4096));
+    recip_kernel<<<blocks, 256, 0, s>>>(src, dst, n);
+    PDFP_CK(cudaGetLastError());
+}
+
 void DeviceMatrix::refresh_f32(cudaStream_t s) {
     if (!v32_a || L.NNZ == 0) return;
     int blocks = static_cast<int>(std::min<int64_t>((L.NNZ + 255) / 256, 4096));

@@ -150,4 +150,18 @@ class DeviceMatrix {
                   Tiling& pairs, std::vector<uint8_t>& is_long) const;
 };
 
+// dst[i] = src[i] rounded to FP32, and dst[i] = 1 / src[i] (correctly rounded), on a stream.
+void cast_f64_to_f32(const double* src, float* dst, int64_t n, cudaStream_t s);
+void reciprocal(const double* src, double* dst, int64_t n, cudaStream_t s);
+
+// scale_problem's arithmetic (src/preconditioner.jl:26-99: Ruiz rounds, Pock-Chambolle
+// with alpha, optionally the bound/objective rescaling) applied in place to an uploaded
+// matrix in the caller's order (both sides), and to the device vectors vin = {c, lb,
+// ub, con_lb, con_ub}, written scaled to vout; D_r, D_c and scales = {bound scale,
+// objective scale} (1 without rescaling) to device memory.  Stream-ordered, no host
+// synchronisation (precond.cu).
+void scale_uploaded(const DeviceMatrix& M, DeviceArena& ar, int32_t ruiz_iterations, double alpha,
+                    bool rescale, const double* const vin[5], double* const vout[5], double* D_r,
+                    double* D_c, double* scales, cudaStream_t st);
+
 }  // namespace pdfp

@@ -414,9 +414,12 @@ __global__ void zero_maxes_kernel(unsigned long long* m) {
 
 class LpSolver {
   public:
-    LpSolver(const pdfp_csr& A, const double* c_s, const double* lb_s, const double* ub_s,
-             const double* clb_s, const double* cub_s, const double* D_r, const double* D_c,
-             double bound_scale, double objective_scale, bool cupdlpx, int precision)
+    // The LP in its original units; it is scaled on the device (scale_uploaded: Ruiz
+    // rounds and Pock-Chambolle alpha, with the bound/objective rescaling), as
+    // solve_lp_relaxation scales it first (src/pdlp.jl:381-393).
+    LpSolver(const pdfp_csr& A, const double* c, const double* lb, const double* ub,
+             const double* clb, const double* cub, int32_t ruiz_iterations, double alpha,
+             bool cupdlpx, int precision)
         : cupdlpx_(cupdlpx), f32_(precision == PDFP_MIXED) {
         int dev = 0;
         PDFP_CK(cudaGetDevice(&dev));
@@ -434,7 +437,7 @@ class LpSolver {
             const int64_t min_nnz = mm ? std::atoll(mm) : (int64_t(1) << 18);
             if (M_.L.NNZ < min_nnz) f32_ = false;
         }
-        M_.upload(ar_, f32_);
+        M_.upload(ar_, f32_);  // unscaled; the FP32 copies are refreshed after the scaling
         {
             const char* te = std::getenv("PDFP_TINY");
             tiny_ = !(te && te[0] == '0') && static_cast<int64_t>(A.m) + A.n <= 4096 &&
@@ -465,25 +468,50 @@ class LpSolver {
             v32_.val_t = M_.v32_t;
             v32_.val_a = M_.v32_a;
         }
-        auto up = [&](double* dst, const double* src, int64_t len) {
-            if (len) PDFP_CK(cudaMemcpy(dst, src, sizeof(double) * len, cudaMemcpyHostToDevice));
-        };
-        up(v64_.c, c_s, n_);
-        up(v64_.lb, lb_s, n_);
-        up(v64_.ub, ub_s, n_);
-        up(v64_.clb, clb_s, m_);
-        up(v64_.cub, cub_s, m_);
-        if (f32_) {
-            auto cast = [&](float* dst, const double* src, int64_t len) {
-                std::vector<float> f(len);
-                for (int64_t i = 0; i < len; ++i) f[i] = static_cast<float>(src[i]);
-                if (len) PDFP_CK(cudaMemcpy(dst, f.data(), sizeof(float) * len, cudaMemcpyHostToDevice));
-            };
-            cast(v32_.c, c_s, n_);
-            cast(v32_.lb, lb_s, n_);
-            cast(v32_.ub, ub_s, n_);
-            cast(v32_.clb, clb_s, m_);
-            cast(v32_.cub, cub_s, m_);
+        // the original vectors in one copy, scaled on the device into the iterate
+        // vectors; D_c and the two scales come back in one copy
+        {
+            const int64_t tot = 3 * int64_t(n_) + 2 * int64_t(m_);
+            std::vector<double> hin(std::max<int64_t>(tot, 1));
+            const double* src[5] = {c, lb, ub, clb, cub};
+            const int64_t len[5] = {n_, n_, n_, m_, m_};
+            double* const din = ar_.alloc<double>(hin.size());
+            const double* vin[5];
+            double* const vout[5] = {v64_.c, v64_.lb, v64_.ub, v64_.clb, v64_.cub};
+            int64_t off = 0;
+            for (int k = 0; k < 5; ++k) {
+                if (len[k]) std::copy(src[k], src[k] + len[k], hin.begin() + off);
+                vin[k] = din + off;
+                off += len[k];
+            }
+            double* dsc = ar_.alloc<double>(static_cast<size_t>(n_) + m_ + 2);  // D_c, D_r, scales
+            double* D_c = dsc;
+            double* D_r = dsc + n_;
+            double* scales = D_r + m_;
+            if (tot) PDFP_CK(cudaMemcpyAsync(din, hin.data(), sizeof(double) * tot, cudaMemcpyHostToDevice, stream_));
+            scale_uploaded(M_, ar_, ruiz_iterations, alpha, true, vin, vout, D_r, D_c, scales, stream_);
+            if (f32_) {
+                M_.refresh_f32(stream_);
+                float* const f[5] = {v32_.c, v32_.lb, v32_.ub, v32_.clb, v32_.cub};
+                for (int k = 0; k < 5; ++k) cast_f64_to_f32(vout[k], f[k], len[k], stream_);
+            }
+            d_.row_unscale = nullptr;
+            d_.col_unscale = nullptr;
+            if (cupdlpx) {  // cupdlpx_termination!, src/pdlp.jl:105-110: 1 ./ D_r, 1 ./ D_c
+                double* dru = ar_.alloc<double>(m_);
+                double* dcu = ar_.alloc<double>(n_);
+                reciprocal(D_r, dru, m_, stream_);
+                reciprocal(D_c, dcu, n_, stream_);
+                d_.row_unscale = dru;
+                d_.col_unscale = dcu;
+            }
+            D_c_.resize(static_cast<size_t>(n_) + 2);
+            PDFP_CK(cudaMemcpyAsync(D_c_.data(), D_c, sizeof(double) * n_, cudaMemcpyDeviceToHost, stream_));
+            PDFP_CK(cudaMemcpyAsync(D_c_.data() + n_, scales, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_));
+            PDFP_CK(cudaStreamSynchronize(stream_));
+            bound_scale_ = D_c_[n_];
+            objective_scale_ = D_c_[n_ + 1];
+            D_c_.resize(n_);
         }
         d_.c = v64_.c;
         d_.lb = v64_.lb;
@@ -499,19 +527,6 @@ class LpSolver {
         d_.maxes = ar_.alloc<unsigned long long>(4);
         ray_part_col_ = ar_.alloc<double>(2 * static_cast<size_t>(std::max(ev_t_.dev.n_tiles, 1)));
         ray_part_row_ = ar_.alloc<double>(static_cast<size_t>(std::max(ev_a_.dev.n_tiles, 1)));
-        d_.row_unscale = nullptr;
-        d_.col_unscale = nullptr;
-        if (cupdlpx) {  // cupdlpx_termination!, src/pdlp.jl:105-110
-            std::vector<double> ru(m_), cu(n_);
-            for (int32_t i = 0; i < m_; ++i) ru[i] = 1.0 / D_r[i];
-            for (int32_t j = 0; j < n_; ++j) cu[j] = 1.0 / D_c[j];
-            double* dru = ar_.alloc<double>(m_);
-            double* dcu = ar_.alloc<double>(n_);
-            up(dru, ru.data(), m_);
-            up(dcu, cu.data(), n_);
-            d_.row_unscale = dru;
-            d_.col_unscale = dcu;
-        }
         st_ = ar_.alloc<InstState>(1);
         flags_ = ar_.alloc<InstFlags>(2);
         err_ = ar_.alloc<int32_t>(4);
@@ -522,8 +537,8 @@ class LpSolver {
         s.best_gap = INFINITY;
         s.fpe = s.initial_fpe = s.last_trial_fpe = INFINITY;
         s.rel_p = s.rel_d = s.rel_gap = INFINITY;
-        s.bound_scale = bound_scale;
-        s.objective_scale = objective_scale;
+        s.bound_scale = bound_scale_;
+        s.objective_scale = objective_scale_;
         s.objective_value = NAN;
         s.nnz_zero = (A.m == 0 || A.row_ptr[A.m] == 0) ? 1 : 0;
         s.mode = f32_ ? MODE_FP32 : MODE_FP64;
@@ -539,6 +554,8 @@ class LpSolver {
 
     int32_t solve(double tolerance, double time_limit, int32_t sv_max_it, double sv_tol,
                   double* x_scaled, double* dual_slack, pdfp_result* r);
+    const std::vector<double>& col_scale() const { return D_c_; }  // D_c, host copy
+    double bound_scale() const { return bound_scale_; }
 
   private:
     template <typename T>
@@ -556,6 +573,8 @@ class LpSolver {
     void prepare_grids();
 
     bool cupdlpx_, f32_;
+    std::vector<double> D_c_;
+    double bound_scale_ = 1.0, objective_scale_ = 1.0;
     bool tiny_ = false;  // small LP: whole windows in one launch (lp_tiny_solve_kernel)
     int sms_ = 148;
     int max_smem_ = 232448;  // dynamic shared memory a block may opt into
@@ -721,6 +740,8 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
     s.kd = 0.0;
     s.ismooth = 0.3;
     s.status = ST_RUNNING;
+    s.best_score = INFINITY;
+    s.stall = 0;
     PDFP_CK(cudaMemcpy(st_, &s, sizeof(s), cudaMemcpyHostToDevice));
     double* part4 = ar_.alloc<double>(4 * static_cast<size_t>(std::max(ev_a_.dev.n_tiles, 1)));
     double* part8 = ar_.alloc<double>(8 * static_cast<size_t>(std::max(ev_t_.dev.n_tiles, 1)));
@@ -729,10 +750,6 @@ int32_t LpSolver::solve(double tolerance, double time_limit, int32_t sv_max_it, 
     launch_finalize(1, LpNormFin{ev_t_.inst_tile0, part8, ev_a_.inst_tile0, part4, st_, cupdlpx_ ? 1 : 0}, stream_);
     PDFP_CK(cudaGetLastError());
 
-    s.best_score = INFINITY;
-    s.stall = 0;
-    PDFP_CK(cudaMemcpy(&st_->best_score, &s.best_score, sizeof(double), cudaMemcpyHostToDevice));
-    PDFP_CK(cudaMemcpy(&st_->stall, &s.stall, sizeof(int32_t), cudaMemcpyHostToDevice));
     // a small LP's window is a dozen launches: issue them directly, with no graph to
     // capture and instantiate per solve; a larger one replays a captured window
     bool f32_window = f32_;
@@ -811,20 +828,13 @@ void solve_lp_relaxation_device(const pdfp_csr& A, const double* c, const double
     // solve_lp_relaxation, src/pdlp.jl:381-393
     if (precision != PDFP_FP64 && precision != PDFP_MIXED) throw Error(E_INVALID, "bad precision");
     const int32_t m = A.m, n = A.n;
-    const int64_t nnz = m > 0 ? A.row_ptr[m] : 0;
     std::vector<double> con_lb(m);
     for (int32_t i = 0; i < m; ++i) con_lb[i] = is_le[i] ? -INFINITY : b[i];
-    std::vector<double> vals(std::max<int64_t>(nnz, 1)), c_s(n), lb_s(n), ub_s(n), D_c(n), clb_s(m),
-        cub_s(m), D_r(m);
-    double bs = 1.0, os = 1.0;
-    scale_problem_device(A, c, l, u, con_lb.data(), b, 10, 1.0, true, vals.data(), c_s.data(),
-                         lb_s.data(), ub_s.data(), clb_s.data(), cub_s.data(), D_r.data(), D_c.data(),
-                         &bs, &os);
-    pdfp_csr As{m, n, A.row_ptr, A.col_idx, vals.data()};
-    LpSolver lp(As, c_s.data(), lb_s.data(), ub_s.data(), clb_s.data(), cub_s.data(), D_r.data(),
-                D_c.data(), bs, os, cupdlpx, precision);
+    LpSolver lp(A, c, l, u, con_lb.data(), b, 10, 1.0, cupdlpx, precision);
     std::vector<double> px(std::max(n, 1));
     lp.solve(tolerance, time_limit, 5000, 1e-4, px.data(), dual_slack_out, r);
+    const std::vector<double>& D_c = lp.col_scale();
+    const double bs = lp.bound_scale();
     for (int32_t j = 0; j < n; ++j) x_out[j] = (D_c[j] * px[j]) / bs;
 }
 

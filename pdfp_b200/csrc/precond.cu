@@ -206,6 +206,57 @@ __global__ void __launch_bounds__(kScaleTinyThreads)
 
 static int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8192))); }
 
+__global__ void fill_kernel(double* __restrict__ d, int64_t n, double v) {
+    for (int64_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += int64_t(gridDim.x) * 256) d[i] = v;
+}
+
+void scale_uploaded(const DeviceMatrix& M, DeviceArena& ar, int32_t ruiz_iterations, double alpha,
+                    bool rescale, const double* const vin[5], double* const vout[5], double* D_r,
+                    double* D_c, double* scales, cudaStream_t st) {
+    const int32_t m = static_cast<int32_t>(M.L.M), n = static_cast<int32_t>(M.L.N);
+    double* rs = ar.alloc<double>(m);
+    double* cs = ar.alloc<double>(n);
+    const int bm = blocks_for(m), bn = blocks_for(n);
+    if (m) fill_kernel<<<bm, 256, 0, st>>>(D_r, m, 1.0);
+    if (n) fill_kernel<<<bn, 256, 0, st>>>(D_c, n, 1.0);
+    fill_kernel<<<1, 256, 0, st>>>(scales, 2, 1.0);
+    auto apply = [&]() {
+        if (m) apply_scale_kernel<<<bm, 256, 0, st>>>(M.rp_a, M.ci_a, M.v64_a, m, rs, cs, 0);
+        if (n) apply_scale_kernel<<<bn, 256, 0, st>>>(M.rp_t, M.ci_t, M.v64_t, n, rs, cs, 1);
+        if (m) mul_inplace_kernel<<<bm, 256, 0, st>>>(D_r, rs, m);
+        if (n) mul_inplace_kernel<<<bn, 256, 0, st>>>(D_c, cs, n);
+    };
+    const char* te = std::getenv("PDFP_TINY");
+    const bool tiny = !(te && te[0] == '0') && static_cast<int64_t>(m) + n <= kScaleTinyMaxDim &&
+                      M.L.NNZ <= kScaleTinyMaxNnz && m > 0 && n > 0;
+    if (tiny) {  // every round in one launch
+        scale_tiny_kernel<<<1, kScaleTinyThreads, 0, st>>>(M.rp_a, M.ci_a, M.v64_a, M.rp_t, M.ci_t,
+                                                           M.v64_t, m, n, std::max(ruiz_iterations, 0),
+                                                           alpha, rs, cs, D_r, D_c);
+    } else {
+        for (int32_t it = 0; it < ruiz_iterations; ++it) {  // src/preconditioner.jl:36-49
+            if (m) ruiz_scale_kernel<<<bm, 256, 0, st>>>(M.rp_a, M.v64_a, m, rs);
+            if (n) ruiz_scale_kernel<<<bn, 256, 0, st>>>(M.rp_t, M.v64_t, n, cs);
+            apply();
+        }
+        // Pock-Chambolle, src/preconditioner.jl:51-64
+        if (m) pc_scale_kernel<<<bm, 256, 0, st>>>(M.rp_a, M.v64_a, m, alpha, rs);
+        if (n) pc_scale_kernel<<<bn, 256, 0, st>>>(M.rp_t, M.v64_t, n, 2.0 - alpha, cs);
+        apply();
+    }
+    // the scaled vectors and the optional bound/objective rescaling
+    double* sq = ar.alloc<double>(2);
+    const int bb = blocks_for(std::max(m, n));
+    scale_vectors_kernel<<<bb, 256, 0, st>>>(vin[0], vin[1], vin[2], D_c, n, vin[3], vin[4], D_r, m,
+                                             vout[0], vout[1], vout[2], vout[3], vout[4]);
+    if (rescale) {
+        rescale_norms_kernel<<<1, 64, 0, st>>>(vin[3], vin[4], vout[3], vout[4], m, vout[0], n, sq);
+        rescale_apply_kernel<<<bb, 256, 0, st>>>(vin[1], vin[2], n, vin[3], vin[4], m, sq, vout[0],
+                                                 vout[1], vout[2], vout[3], vout[4], scales);
+    }
+    PDFP_CK(cudaGetLastError());
+}
+
 void scale_problem_device(const pdfp_csr& A, const double* c, const double* var_lb,
                           const double* var_ub, const double* con_lb, const double* con_ub,
                           int32_t ruiz_iterations, double alpha, bool rescale, double* val_out,
@@ -220,72 +271,42 @@ void scale_problem_device(const pdfp_csr& A, const double* c, const double* var_
     if (!msg.empty()) throw Error(E_INVALID, msg);
     DeviceArena ar;
     M.upload(ar, false);
-    double* D_r = ar.alloc<double>(m);
-    double* D_c = ar.alloc<double>(n);
-    double* rs = ar.alloc<double>(m);
-    double* cs = ar.alloc<double>(n);
-    std::vector<double> ones_m(m, 1.0), ones_n(n, 1.0);
-    if (m) PDFP_CK(cudaMemcpy(D_r, ones_m.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
-    if (n) PDFP_CK(cudaMemcpy(D_c, ones_n.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    const int bm = blocks_for(m), bn = blocks_for(n);
-    auto apply = [&]() {
-        if (m) apply_scale_kernel<<<bm, 256>>>(M.rp_a, M.ci_a, M.v64_a, m, rs, cs, 0);
-        if (n) apply_scale_kernel<<<bn, 256>>>(M.rp_t, M.ci_t, M.v64_t, n, rs, cs, 1);
-        if (m) mul_inplace_kernel<<<bm, 256>>>(D_r, rs, m);
-        if (n) mul_inplace_kernel<<<bn, 256>>>(D_c, cs, n);
-    };
-    const char* te = std::getenv("PDFP_TINY");
-    const bool tiny = !(te && te[0] == '0') && static_cast<int64_t>(m) + n <= kScaleTinyMaxDim &&
-                      M.L.NNZ <= kScaleTinyMaxNnz && m > 0 && n > 0;
-    if (tiny) {  // every round in one launch
-        scale_tiny_kernel<<<1, kScaleTinyThreads>>>(M.rp_a, M.ci_a, M.v64_a, M.rp_t, M.ci_t, M.v64_t,
-                                                    m, n, std::max(ruiz_iterations, 0), alpha, rs, cs,
-                                                    D_r, D_c);
-    } else {
-        for (int32_t it = 0; it < ruiz_iterations; ++it) {  // src/preconditioner.jl:36-49
-            if (m) ruiz_scale_kernel<<<bm, 256>>>(M.rp_a, M.v64_a, m, rs);
-            if (n) ruiz_scale_kernel<<<bn, 256>>>(M.rp_t, M.v64_t, n, cs);
-            apply();
-        }
-        // Pock-Chambolle, src/preconditioner.jl:51-64
-        if (m) pc_scale_kernel<<<bm, 256>>>(M.rp_a, M.v64_a, m, alpha, rs);
-        if (n) pc_scale_kernel<<<bn, 256>>>(M.rp_t, M.v64_t, n, 2.0 - alpha, cs);
-        apply();
-    }
-    PDFP_CK(cudaGetLastError());
-    PDFP_CK(cudaDeviceSynchronize());
-
-    // scaled vectors and the optional bound/objective rescaling, on the device
-    const int64_t nnz = M.L.NNZ;
-    double* dv[10];
-    const double* hin[5] = {c, var_lb, var_ub, con_lb, con_ub};
+    // inputs in one block: c, lb, ub (n each), con_lb, con_ub (m each), then the outputs,
+    // D_c, D_r and the two scales
+    const int64_t tot = 3 * int64_t(n) + 2 * int64_t(m);
+    std::vector<double> hin(std::max<int64_t>(tot, 1));
+    const double* src[5] = {c, var_lb, var_ub, con_lb, con_ub};
     const int64_t len[5] = {n, n, n, m, m};
+    double* const din = ar.alloc<double>(hin.size());
+    double* const dout = ar.alloc<double>(tot + n + m + 2);
+    const double* vin[5];
+    double* vout[5];
+    int64_t off = 0;
     for (int k = 0; k < 5; ++k) {
-        dv[k] = ar.alloc<double>(len[k]);
-        if (len[k]) PDFP_CK(cudaMemcpy(dv[k], hin[k], sizeof(double) * len[k], cudaMemcpyHostToDevice));
+        if (len[k]) std::copy(src[k], src[k] + len[k], hin.begin() + off);
+        vin[k] = din + off;
+        vout[k] = dout + off;
+        off += len[k];
     }
-    for (int k = 5; k < 10; ++k) dv[k] = ar.alloc<double>(len[k - 5]);
-    double* sq = ar.alloc<double>(4);
-    const int bb = blocks_for(std::max(m, n));
-    scale_vectors_kernel<<<bb, 256>>>(dv[0], dv[1], dv[2], D_c, n, dv[3], dv[4], D_r, m, dv[5],
-                                      dv[6], dv[7], dv[8], dv[9]);
-    double scales[2] = {1.0, 1.0};
-    if (rescale) {
-        rescale_norms_kernel<<<1, 64>>>(dv[3], dv[4], dv[8], dv[9], m, dv[5], n, sq);
-        rescale_apply_kernel<<<bb, 256>>>(dv[1], dv[2], n, dv[3], dv[4], m, sq, dv[5], dv[6], dv[7],
-                                          dv[8], dv[9], sq + 2);
-    }
-    PDFP_CK(cudaGetLastError());
+    double* D_c = dout + tot;
+    double* D_r = D_c + n;
+    double* scales = D_r + m;
+    if (tot) PDFP_CK(cudaMemcpy(din, hin.data(), sizeof(double) * tot, cudaMemcpyHostToDevice));
+    scale_uploaded(M, ar, ruiz_iterations, alpha, rescale, vin, vout, D_r, D_c, scales, 0);
     PDFP_CK(cudaDeviceSynchronize());
-    if (rescale) PDFP_CK(cudaMemcpy(scales, sq + 2, sizeof(scales), cudaMemcpyDeviceToHost));
-    if (nnz) PDFP_CK(cudaMemcpy(val_out, M.v64_a, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
-    double* hout[7] = {c_out, var_lb_out, var_ub_out, con_lb_out, con_ub_out, D_c_out, D_r_out};
-    const double* dsrc[7] = {dv[5], dv[6], dv[7], dv[8], dv[9], D_c, D_r};
-    const int64_t olen[7] = {n, n, n, m, m, n, m};
-    for (int k = 0; k < 7; ++k)
-        if (olen[k]) PDFP_CK(cudaMemcpy(hout[k], dsrc[k], sizeof(double) * olen[k], cudaMemcpyDeviceToHost));
-    *bound_scale = scales[0];
-    *objective_scale = scales[1];
+    std::vector<double> hout(tot + n + m + 2);
+    PDFP_CK(cudaMemcpy(hout.data(), dout, sizeof(double) * hout.size(), cudaMemcpyDeviceToHost));
+    if (M.L.NNZ) PDFP_CK(cudaMemcpy(val_out, M.v64_a, sizeof(double) * M.L.NNZ, cudaMemcpyDeviceToHost));
+    double* dst[5] = {c_out, var_lb_out, var_ub_out, con_lb_out, con_ub_out};
+    off = 0;
+    for (int k = 0; k < 5; ++k) {
+        if (len[k]) std::copy(hout.begin() + off, hout.begin() + off + len[k], dst[k]);
+        off += len[k];
+    }
+    if (n) std::copy(hout.begin() + tot, hout.begin() + tot + n, D_c_out);
+    if (m) std::copy(hout.begin() + tot + n, hout.begin() + tot + n + m, D_r_out);
+    *bound_scale = hout[tot + n + m];
+    *objective_scale = hout[tot + n + m + 1];
 }
 
 double estimate_sv_device(const pdfp_csr& A, int32_t max_iterations, double tolerance,
