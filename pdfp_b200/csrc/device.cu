@@ -128,18 +128,26 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ a, float* __restric
         b[i] = static_cast<float>(a[i]);
 }
 
+template <class T>
+static std::pair<const void*, size_t> part(const std::vector<T>& v) {
+    return {v.data(), v.size() * sizeof(T)};
+}
+
 void DeviceMatrix::upload(DeviceArena& ar, bool want_f32) {
-    rp_a = ar.upload(L.A.rp);
-    ci_a = ar.upload(L.A.ci);
-    v64_a = ar.upload(L.A.v);
-    rp_t = ar.upload(L.At.rp);
-    ci_t = ar.upload(L.At.ci);
-    v64_t = ar.upload(L.At.v);
-    row_off = ar.upload(L.row_off);
-    col_off = ar.upload(L.col_off);
-    n_eq = ar.upload(L.n_eq);
-    row_orig = ar.upload(L.row_orig);
-    col_orig = ar.upload(L.col_orig);
+    const std::vector<void*> d = ar.upload_group(
+        {part(L.A.rp), part(L.A.ci), part(L.A.v), part(L.At.rp), part(L.At.ci), part(L.At.v),
+         part(L.row_off), part(L.col_off), part(L.n_eq), part(L.row_orig), part(L.col_orig)});
+    rp_a = static_cast<int32_t*>(d[0]);
+    ci_a = static_cast<int32_t*>(d[1]);
+    v64_a = static_cast<double*>(d[2]);
+    rp_t = static_cast<int32_t*>(d[3]);
+    ci_t = static_cast<int32_t*>(d[4]);
+    v64_t = static_cast<double*>(d[5]);
+    row_off = static_cast<int32_t*>(d[6]);
+    col_off = static_cast<int32_t*>(d[7]);
+    n_eq = static_cast<int32_t*>(d[8]);
+    row_orig = static_cast<int32_t*>(d[9]);
+    col_orig = static_cast<int32_t*>(d[10]);
     max_m = max_n = 0;
     for (int p = 0; p < L.K; ++p) {
         max_m = std::max(max_m, L.row_off[p + 1] - L.row_off[p]);
@@ -191,9 +199,6 @@ static DeviceMatrix::Tiling upload_tiling(DeviceArena& ar, DeviceMatrix::Tiling&
     s.stage_bytes = g.stage_bytes;
     s.rp = rp;
     s.ci = ci;
-    s.tile_row = ar.upload(t.host.tile_row);
-    s.tile_chunk = ar.upload(t.host.tile_chunk);
-    s.tile_inst = ar.upload(t.host.tile_inst);
     std::vector<ChunkDesc> desc(t.host.chunk_k0.size());
     for (size_t c = 0; c < desc.size(); ++c) {
         const int32_t tile = t.host.chunk_tile[c];
@@ -201,8 +206,14 @@ static DeviceMatrix::Tiling upload_tiling(DeviceArena& ar, DeviceMatrix::Tiling&
                             t.host.tile_row_end[tile], tile, t.host.tile_inst[tile],
                             t.host.chunk_flags[c], t.host.tile_chunk[tile] == (int32_t)c ? 1 : 0};
     }
-    s.chunks = ar.upload(desc);
-    t.inst_tile0 = ar.upload(t.host.inst_tile0);
+    const std::vector<void*> d = ar.upload_group({part(t.host.tile_row), part(t.host.tile_chunk),
+                                                  part(t.host.tile_inst), part(desc),
+                                                  part(t.host.inst_tile0)});
+    s.tile_row = static_cast<const int32_t*>(d[0]);
+    s.tile_chunk = static_cast<const int32_t*>(d[1]);
+    s.tile_inst = static_cast<const int32_t*>(d[2]);
+    s.chunks = static_cast<const ChunkDesc*>(d[3]);
+    t.inst_tile0 = static_cast<int32_t*>(d[4]);
     return std::move(t);
 }
 

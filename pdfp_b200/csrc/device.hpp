@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -82,6 +83,38 @@ class DeviceArena {
         T* d = alloc<T>(h.size());
         if (!h.empty()) PDFP_CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
         return d;
+    }
+    // Several host arrays {pointer, bytes} uploaded with one copy when together they
+    // take at most kGroupBytes: each gets its own 256-byte aligned, 64-byte padded,
+    // zero-filled region of one allocation (the layout alloc() gives separate
+    // buffers); larger groups go one array at a time.  A small handle's dozens of
+    // arrays then cost one host-to-device copy instead of one each.
+    static constexpr size_t kGroupBytes = size_t(8) << 20;
+    std::vector<void*> upload_group(const std::vector<std::pair<const void*, size_t>>& parts) {
+        std::vector<void*> out(parts.size(), nullptr);
+        std::vector<size_t> off(parts.size());
+        size_t total = 0;
+        for (size_t i = 0; i < parts.size(); ++i) {
+            off[i] = total;
+            total = (total + parts[i].second + 64 + 255) & ~size_t(255);
+        }
+        if (total > kGroupBytes) {
+            for (size_t i = 0; i < parts.size(); ++i) {
+                unsigned char* d = alloc<unsigned char>(parts[i].second);
+                if (parts[i].second)
+                    PDFP_CK(cudaMemcpy(d, parts[i].first, parts[i].second, cudaMemcpyHostToDevice));
+                out[i] = d;
+            }
+            return out;
+        }
+        unsigned char* d = alloc<unsigned char>(total);
+        std::vector<unsigned char> h(total, 0);
+        for (size_t i = 0; i < parts.size(); ++i) {
+            if (parts[i].second) std::memcpy(h.data() + off[i], parts[i].first, parts[i].second);
+            out[i] = d + off[i];
+        }
+        if (total) PDFP_CK(cudaMemcpy(d, h.data(), total, cudaMemcpyHostToDevice));
+        return out;
     }
     void release() {
         if (!ptrs_.empty()) arena_free(ptrs_, pooled_);
