@@ -172,6 +172,20 @@ PDFP_API int pdfp_solve(pdfp_handle* h, const pdfp_params* p, double primal_weig
  * primal_weights and results hold one entry per instance. */
 PDFP_API int pdfp_solve_batch(pdfp_handle* h, const pdfp_params* params, const double* primal_weights,
                      pdfp_result* results);
+/* pdfp_solve! for the members of a batch handle, returning as soon as at least one
+ * member that was running has stopped (checked at evaluation-window boundaries);
+ * the others stop at their next window boundary and report status 0 (still
+ * running).  A later call with resume[p] != 0 continues member p exactly where it
+ * stopped (its tolerances, limits, restart state and counters stand; params[p] is
+ * not read for it); members with resume[p] == 0 (or resume == NULL) start a new
+ * solve as in pdfp_solve_batch.  Resuming a member that is not running from the
+ * previous call, or after pdfp_set_target / pdfp_warm_start on it, is an error.
+ * This lets concurrent pump trajectories each advance at their own pace, as the
+ * reference's separate pump processes do (scripts/solve.jl:121-148), instead of
+ * every pump iteration waiting for the slowest member's projection. */
+PDFP_API int pdfp_solve_batch_any(pdfp_handle* h, const pdfp_params* params,
+                                  const double* primal_weights, const uint8_t* resume,
+                                  pdfp_result* results);
 /* Read a state vector of an instance (s.pdhg_x etc., scaled units, the
  * caller's variable/row order). */
 PDFP_API int pdfp_get_vector(pdfp_handle* h, int32_t instance, int32_t which, double* out);

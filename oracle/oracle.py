@@ -367,5 +367,12 @@ class OracleSolvers:
                 self.results[p] = dict(s.last)
             return out
 
+        def solve_any(self, params, primal_weights, resume=None):
+            # the oracle's members are solved one after the other, each to the end:
+            # every member stops in the call, so none is ever left to resume
+            if resume is not None and any(resume):
+                raise ValueError("no oracle member is left running between calls")
+            return self.solve(params, primal_weights)
+
         def get(self, p, which):
             return self.members[p].get(which)

@@ -99,6 +99,7 @@ SIGNATURES = {
     "pdfp_warm_start": (C.c_int, [vp, C.c_int32]),
     "pdfp_solve": (C.c_int, [vp, C.POINTER(Params), C.c_double, C.POINTER(Result)]),
     "pdfp_solve_batch": (C.c_int, [vp, C.POINTER(Params), dp, C.POINTER(Result)]),
+    "pdfp_solve_batch_any": (C.c_int, [vp, C.POINTER(Params), dp, up, C.POINTER(Result)]),
     "pdfp_get_vector": (C.c_int, [vp, C.c_int32, C.c_int32, dp]),
     "pdfp_get_x": (C.c_int, [vp, C.c_int32, dp]),
     "pdfp_set_col_scale": (C.c_int, [vp, C.c_int32, dp]),

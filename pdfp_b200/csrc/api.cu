@@ -182,6 +182,14 @@ int pdfp_solve_batch(pdfp_handle* h, const pdfp_params* params, const double* pr
     });
 }
 
+int pdfp_solve_batch_any(pdfp_handle* h, const pdfp_params* params, const double* primal_weights,
+                         const uint8_t* resume, pdfp_result* results) {
+    return guarded([&] {
+        if (!h || !params || !primal_weights || !results) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        h->proj->solve(params, primal_weights, results, resume, true);
+    });
+}
+
 int pdfp_get_vector(pdfp_handle* h, int32_t instance, int32_t which, double* out) {
     return guarded([&] {
         if (!h || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");

@@ -38,9 +38,9 @@ constexpr int32_t kHostNanScanMax = 1 << 16;  // vectors up to this length are c
 
 // ---- per-instance state kernels ---------------------------------------------------
 
-__global__ void solve_begin_kernel(InstState* st, int K) {
+__global__ void solve_begin_kernel(InstState* st, const SolveParams* sp, int K) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < K) st[p].t_start_ns = globaltimer_ns();
+    if (p < K && !sp[p].resume) st[p].t_start_ns = globaltimer_ns();
 }
 
 __global__ void set_max_sv_kernel(InstState* st, const double* sv, int K) {
@@ -55,6 +55,10 @@ __global__ void solve_init_kernel(InstState* st, InstFlags* fl, const SolveParam
     if (p >= K) return;
     InstState& s = st[p];
     const SolveParams& q = sp[p];
+    if (q.resume) {  // running from an earlier call: its parameters and counters stand
+        fl[p] = InstFlags{s.status, s.mode, 0, 0};
+        return;
+    }
     s.eps_opt = q.eps_opt;
     s.eps_feas = q.eps_feas;
     s.time_limit = q.time_limit;
@@ -300,7 +304,7 @@ __global__ void __launch_bounds__(kTinyThreads)
                       const int32_t* __restrict__ g_rp_a, const int32_t* __restrict__ g_ci_a,
                       const int32_t* __restrict__ col_off, const int32_t* __restrict__ row_off,
                       const int32_t* __restrict__ n_eq, int32_t* err, int32_t max_windows,
-                      int32_t polish, int32_t rowsum_len) {
+                      int32_t polish, int32_t rowsum_len, int32_t* any_stop) {
     constexpr int NT = kTinyThreads;
     constexpr int32_t mode = std::is_same<T, float>::value ? MODE_FP32 : MODE_FP64;
     extern __shared__ __align__(16) double tiny_rowsum[];  // rowsum_len doubles, then the staged copy
@@ -420,7 +424,11 @@ __global__ void __launch_bounds__(kTinyThreads)
         __syncthreads();
     };
     for (int32_t w = 0; w < max_windows; ++w) {
-        if (threadIdx.x == 0) go = st[p].status == ST_RUNNING && st[p].mode == mode;
+        // any_stop (a solve that returns once any member stops): after another
+        // member's block has stopped, leave at this window boundary, still running
+        if (threadIdx.x == 0)
+            go = st[p].status == ST_RUNNING && st[p].mode == mode &&
+                 !(any_stop && *reinterpret_cast<volatile int32_t*>(any_stop));
         __syncthreads();
         if (!go) break;
         const int32_t freq = st[p].freq;
@@ -441,7 +449,10 @@ __global__ void __launch_bounds__(kTinyThreads)
         const RestartCopy<T> rc{v, st, col_off, row_off, mode};
         if (rc.active(p))
             for (int32_t i = threadIdx.x; i < (c1 - c0) + (r1 - r0); i += NT) rc.elem(p, i);
-        if (threadIdx.x == 0) go = st[p].status == ST_RUNNING && !fl[p].polish_request;
+        if (threadIdx.x == 0) {
+            go = st[p].status == ST_RUNNING && !fl[p].polish_request;
+            if (any_stop && st[p].status != ST_RUNNING) atomicExch(any_stop, 1);
+        }
         __syncthreads();
         if (!go) break;
     }
@@ -689,6 +700,8 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
     flags_h_ = static_cast<InstFlags*>(pinned_take(sizeof(InstFlags) * (K_ + 1)));
     st_h_ = static_cast<InstState*>(pinned_take(sizeof(InstState) * K_));
     host_total_.assign(K_, 0);
+    last_running_.assign(K_, 0);
+    any_stop_ = ar_.alloc<int32_t>(4);
     nan_seen_h_ = static_cast<int32_t*>(pinned_take(sizeof(int32_t)));
     vec_mode_.assign(K_, precision_ == PDFP_MIXED ? MODE_FP32 : MODE_FP64);
 
@@ -1407,6 +1420,7 @@ void Projector::warm_start(int p) {
         launch_elem(K_, len, WarmStartCopy<double>{v64_, M_.col_off, M_.row_off, p}, stream_);
     warm_start_state_kernel<<<1, 1, 0, stream_>>>(st_, p);
     host_total_[p] = 0;
+    last_running_[p] = 0;  // a new projection: it starts afresh, it does not resume
     PDFP_CK(cudaGetLastError());  // stream-ordered before the next solve; no host wait
 }
 
@@ -1678,7 +1692,8 @@ void Projector::run_window(int freq, bool with32, bool with64) {
         auto launch = [&](auto kern, auto& vecs, size_t bytes) {
             kern<<<K_, kTinyThreads, bytes, stream_>>>(vecs, ed_, st_, flags_, M_.rp_t, M_.ci_t, M_.rp_a,
                                                        M_.ci_a, M_.col_off, M_.row_off, M_.n_eq, err_,
-                                                       kTinyWindowsPerLaunch, polish_enabled_, rowsum_len);
+                                                       kTinyWindowsPerLaunch, polish_enabled_, rowsum_len,
+                                                       any_stop_cur_);
         };
         if (with32) {
             if (tiny_staged32_) launch(tiny_solve_kernel<float, true>, v32_, tiny_smem32_);
@@ -1719,8 +1734,13 @@ cudaGraphExec_t Projector::window_graph(int freq, bool with32, bool with64) {
     return exec;
 }
 
-void Projector::solve(const pdfp_params* params, const double* primal_weights, pdfp_result* results) {
+void Projector::solve(const pdfp_params* params, const double* primal_weights, pdfp_result* results,
+                      const uint8_t* resume, bool any) {
     auto wall0 = std::chrono::steady_clock::now();
+    for (int p = 0; p < K_ && resume; ++p)
+        if (resume[p] && !last_running_[p])
+            throw Error(E_INVALID, "instance " + std::to_string(p) +
+                                       " cannot resume: it is not running from an earlier call");
     // validate and stage the parameters
     std::vector<SolveParams> sp(K_);
     int freq = -1;
@@ -1759,12 +1779,15 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         s.mode = precision_ == PDFP_MIXED && (stall_limit_ > 0 || !tight) ? MODE_FP32 : MODE_FP64;
         s.stall_limit = stall_limit_;
         s.fp32_floor = fp32_floor_;
+        s.resume = resume && resume[p] ? 1 : 0;
+        if (s.resume) s.mode = vec_mode_[p];  // it keeps its form (FP32 or the polish)
         sv_it = q.sv_max_iterations;
         sv_tol = q.sv_tolerance;
         max_time = std::max(max_time, q.time_limit);
     }
     PDFP_CK(cudaEventRecord(sev_[0], stream_));
-    solve_begin_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, K_);
+    PDFP_CK(cudaMemcpyAsync(sp_, sp.data(), sizeof(SolveParams) * K_, cudaMemcpyHostToDevice, stream_));
+    solve_begin_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, sp_, K_);
     PDFP_CK(cudaGetLastError());
     ensure_step_sizes(sv_it, sv_tol);
     // a mixed handle starts each instance in the mode chosen above: convert the
@@ -1783,7 +1806,6 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
             vec_mode_[p] = sp[p].mode;
         }
     }
-    PDFP_CK(cudaMemcpyAsync(sp_, sp.data(), sizeof(SolveParams) * K_, cudaMemcpyHostToDevice, stream_));
     solve_init_kernel<<<(K_ + 127) / 128, 128, 0, stream_>>>(st_, flags_, sp_, K_);
     launch_rows(ev_t_.dev, DenRows{v64_.w, v64_.xt, part_col_}, stream_);
     launch_finalize(K_, DenFin{ev_t_.inst_tile0, part_col_, nullptr, nullptr, st_}, stream_);
@@ -1795,7 +1817,8 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     // is needed; after a call that advanced the state otherwise, read it back.
     if (totals_known_) {
         for (int p = 0; p < K_; ++p)
-            flags_h_[p] = InstFlags{host_total_[p] < sp[p].iter_limit ? ST_RUNNING : ST_ITERATION_LIMIT,
+            flags_h_[p] = InstFlags{sp[p].resume || host_total_[p] < sp[p].iter_limit ? ST_RUNNING
+                                                                                     : ST_ITERATION_LIMIT,
                                     sp[p].mode, 0, 0};
     } else {
         PDFP_CK(cudaMemcpyAsync(flags_h_, flags_, sizeof(InstFlags) * K_, cudaMemcpyDeviceToHost, stream_));
@@ -1806,6 +1829,12 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
     double kp_sum = 0.0, kd_sum = 0.0;
     int64_t k_samples = 0;
     const TimingPlan plan = timing_plan(freq);
+    // any: return at the first window boundary after an instance that was running
+    // has stopped; the whole-window kernel's blocks leave at theirs too (any_stop)
+    std::vector<uint8_t> started(K_);
+    for (int p = 0; p < K_; ++p) started[p] = flags_h_[p].status == ST_RUNNING;
+    if (any) PDFP_CK(cudaMemsetAsync(any_stop_, 0, sizeof(int32_t), stream_));
+    any_stop_cur_ = any ? any_stop_ : nullptr;
     for (;;) {
         bool running = false;
         for (int p = 0; p < K_; ++p) running = running || flags_h_[p].status == ST_RUNNING;
@@ -1851,8 +1880,17 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
             }
         }
         const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
-        if (wall > max_time + 120.0) throw Error(E_TIMEOUT, "solve exceeded its time limit by 120 s on the host clock");
+        if (wall > max_time + 120.0) {
+            any_stop_cur_ = nullptr;
+            throw Error(E_TIMEOUT, "solve exceeded its time limit by 120 s on the host clock");
+        }
+        if (any) {
+            bool stopped = false;
+            for (int p = 0; p < K_; ++p) stopped = stopped || (started[p] && flags_h_[p].status != ST_RUNNING);
+            if (stopped) break;
+        }
     }
+    any_stop_cur_ = nullptr;
     if (!polled) {
         PDFP_CK(cudaMemcpyAsync(st_h_, st_, sizeof(InstState) * K_, cudaMemcpyDeviceToHost, stream_));
         PDFP_CK(cudaEventRecord(sev_[1], stream_));
@@ -1885,9 +1923,11 @@ void Projector::solve(const pdfp_params* params, const double* primal_weights, p
         r.kernel_samples = k_samples;
         vec_mode_[p] = s.mode;
         host_total_[p] = s.total;
+        last_running_[p] = s.status == ST_RUNNING ? 1 : 0;
     }
     totals_known_ = true;
-    polished_.clear();
+    for (int p = 0; p < K_; ++p)  // a polished instance that keeps running stays marked
+        if (!last_running_[p]) polished_.erase(p);
 }
 
 void Projector::profile_step(int iterations, float* ms_primal, float* ms_dual, double* bytes_primal,

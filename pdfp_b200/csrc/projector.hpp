@@ -45,7 +45,12 @@ class Projector {
     void set_x(int p, const double* x, bool unscaled = false);
     void set_target(int p, const double* xt, bool unscaled = false);
     void warm_start(int p);
-    void solve(const pdfp_params* params, const double* primal_weights, pdfp_result* results);
+    // any = false: until every instance has stopped.  any = true: until at least one
+    // instance that was running has stopped (at a window boundary); the others keep
+    // running, and a later call with resume[p] set continues instance p from there
+    // (its parameters and counters as they were; params[p] is then not read).
+    void solve(const pdfp_params* params, const double* primal_weights, pdfp_result* results,
+               const uint8_t* resume = nullptr, bool any = false);
     void get_vector(int p, int which, double* out, bool unscaled = false);
     void profile_step(int iterations, float* ms_primal, float* ms_dual, double* bytes_primal,
                       double* bytes_dual);
@@ -163,6 +168,9 @@ class Projector {
     InstFlags* flags_h_ = nullptr;
     InstState* st_h_ = nullptr;       // page-locked copy of the states, read with each poll
     std::vector<int64_t> host_total_;  // PDHG iterations per instance as of the last solve
+    std::vector<uint8_t> last_running_;  // still running when the last solve returned
+    int32_t* any_stop_ = nullptr;      // device flag: an instance stopped (any-solves)
+    int32_t* any_stop_cur_ = nullptr;  // any_stop_ during an any-solve, else null
     bool totals_known_ = true;         // host_total_ matches the device
     int32_t* err_ = nullptr;
     SolveParams* sp_ = nullptr;

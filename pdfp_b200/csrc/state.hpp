@@ -48,7 +48,8 @@ struct SolveParams {
     double fp32_floor;
     int64_t iter_limit;
     int32_t freq, mode;
-    int32_t stall_limit, pad;
+    int32_t stall_limit;
+    int32_t resume;  // 1: the instance is running from an earlier call; keep its state
 };
 
 // What the host polls after every window.

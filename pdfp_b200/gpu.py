@@ -276,6 +276,29 @@ class PDFPBatch:
         self.results = [r.as_dict() for r in rs]
         return [r["status"] for r in self.results]
 
+    def solve_any(self, params, primal_weights, resume=None):
+        """pdfp_solve_batch_any: solve until at least one running member stops.
+
+        Members still running when it returns report "RUNNING"; pass resume[p] =
+        True on the next call to continue member p where it stopped (its params
+        entry is then not read).  Returns the members' statuses."""
+        if isinstance(params, SolverParameters):
+            params = [params] * self.k
+        ps = (L.Params * self.k)(*[L.make_params(p) for p in params])
+        pw = L.f64(np.broadcast_to(np.asarray(primal_weights, dtype=np.float64), (self.k,)))
+        rs = (L.Result * self.k)()
+        rz = None
+        if resume is not None:
+            rz = np.ascontiguousarray(np.broadcast_to(np.asarray(resume, dtype=bool), (self.k,)),
+                                      dtype=np.uint8)
+        L.check(L.lib().pdfp_solve_batch_any(self._h, ps, L.dptr(pw),
+                                             L.uptr(rz) if rz is not None else None, rs))
+        self.results = [r.as_dict() for r in rs]
+        for d in self.results:
+            if d["status"] == "UNSPECIFIED":
+                d["status"] = "RUNNING"
+        return [d["status"] for d in self.results]
+
     def get(self, p: int, which: str, out=None) -> np.ndarray:
         m, n = self.shapes[p]
         size = m if which.endswith("_z") else n

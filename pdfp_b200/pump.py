@@ -517,7 +517,7 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
                              push_threshold: float = 0.01, violation_threshold: float = 5000.0,
                              propagation_budget: int = 100_000,
                              feasibility_tolerance: float = 1e-6, precision: str = "fp64",
-                             solvers=None, stop=None):
+                             solvers=None, stop=None, asynchronous: bool = False):
     """Concurrent pump trajectories as members of one batched projector.
 
     Replaces the reference's K concurrent pump processes (scripts/solve.jl:121-148,
@@ -533,6 +533,14 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
     iteration with this process's own verdict (a trajectory succeeded or the time
     ran out) and decides whether to stop; the sharded driver uses it to agree on
     stopping across ranks.
+
+    ``asynchronous=False`` runs the trajectories in lockstep: every pump iteration
+    projects all of them and waits for the slowest.  ``asynchronous=True`` lets each
+    trajectory advance at its own pace, as the reference's separate processes do:
+    the batched projection returns as soon as one member's projection ends
+    (``solve_any``), that trajectory rounds and asks for its next projection, and
+    the others continue where they stopped.  Each trajectory takes exactly the
+    steps it takes in lockstep; only which one finishes first, in time, can differ.
     """
     if batch_policy not in ("cost", "always"):
         raise ValueError("batch_policy must be 'cost' or 'always'")
@@ -595,8 +603,129 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
                                 eps_feasible_relative=gaps[p] * residual_ratio,
                                 time_limit=remaining())
 
+    def after_projection(p, xp, inner_p):
+        """Trajectory p's steps after its projection xp (src/pump.jl:357-406): the
+        tolerance schedule, the success test, rounding, flips and restarts.  True
+        when the projection rounds to a feasible point."""
+        tr = trajs[p]
+        tr.pdhg += inner_p
+        if gaps[p] > gap_floor:
+            gaps[p] = max(gaps[p] * gap_decay, gap_floor)
+        if is_integral(xp, int_idx, tol):
+            cand = _round_to_nearest(xp, milp)
+            if viol(cand) <= tol:
+                tr.found, tr.x_found, tr.t_found = True, cand, elapsed()
+                return True
+        t = time.time()
+        x_round = round_guarded(tr.rounder, xp, tr.rng, tr.iterations)
+        stats.rounding_time += time.time() - t
+        candidate = tr.xt.copy()
+        if _differs(x_round, tr.xt, int_idx):
+            candidate[:] = x_round
+        else:
+            flips = int(tr.rng.integers(flip_parameter // 2, 3 * flip_parameter // 2 + 1))
+            _flip_farthest(candidate, xp, milp, flips)
+        h_candidate = _hash_integers(candidate, int_idx)
+        cycled = h_candidate in tr.seen
+        periodic = tr.since_restart >= restart_period
+        if cycled or periodic:
+            _perturb(candidate, xp, milp, tr.rng, tr.general, tr.is_general, tr.ladder,
+                     tr.iterations)
+            tr.perturbations += 1
+            tr.since_restart = 0
+            for _ in range(10):
+                h = _hash_integers(candidate, int_idx)
+                if not (h in tr.seen or h == tr.h_current):
+                    break
+                _perturb(candidate, xp, milp, tr.rng, tr.general, tr.is_general, tr.ladder,
+                         tr.iterations)
+        tr.seen.add(tr.h_current)
+        tr.h_current = _hash_integers(candidate, int_idx) if (cycled or periodic) else h_candidate
+        tr.xt = candidate
+        return False
+
     winner = None
-    while True:
+
+    def trajectory(p):
+        """Trajectory p as a generator: yields once per projection it needs, with its
+        target (or warm start) already set on member p, and returns True when it
+        found a feasible point (False when the time ran out)."""
+        tr = trajs[p]
+        while True:
+            if viol(tr.xt) <= tol and is_integral(tr.xt, int_idx, tol):
+                tr.found, tr.x_found, tr.t_found = True, tr.xt.copy(), elapsed()
+                return True
+            if elapsed() >= time_limit:
+                return False
+            tr.iterations += 1
+            tr.since_restart += 1
+            scalings[p].set_target(tr.xt)
+            yield
+            xp = scalings[p].x()
+            inner_p = batch.results[p]["total_count"]
+            # mixed models: tenfold tighter re-solves (src/pump.jl:343-356)
+            while mixed and elapsed() < time_limit:
+                if not (budgets[p] > 1e-6 and is_integral(xp, int_idx, tol)
+                        and viol(_round_to_nearest(xp, milp)) > tol):
+                    break
+                budgets[p] *= 0.1
+                gaps[p] = max(gaps[p] * 0.1, 1e-8)
+                batch.warm_start(p)
+                yield
+                xp = scalings[p].x()
+                inner_p += batch.results[p]["total_count"]
+            if after_projection(p, xp, inner_p):
+                return True
+
+    if asynchronous:
+        # the first roundings as the lockstep loop tests them, before any projection
+        for p, tr in enumerate(trajs):
+            if viol(tr.xt) <= tol and is_integral(tr.xt, int_idx, tol):
+                tr.found, tr.x_found, tr.t_found = True, tr.xt.copy(), elapsed()
+                winner = p
+                break
+        gens, want, running = [], [False] * K, set()
+
+        def advance(p):  # run trajectory p to its next projection; True: it succeeded
+            try:
+                next(gens[p])
+                want[p] = True
+                return False
+            except StopIteration as e:
+                want[p] = False
+                return bool(e.value)
+
+        if winner is None:
+            batch, scalings = build_batch()
+            gens = [trajectory(p) for p in range(K)]
+            for p in range(K):
+                if advance(p):
+                    winner = p
+                    break
+        while winner is None:
+            done = elapsed() >= time_limit
+            if (stop(done) if stop is not None else done):
+                break
+            new = [p for p in range(K) if want[p]]
+            if not new and not running:
+                break  # every trajectory ran out of time
+            # members starting a projection get their parameters; running ones
+            # resume (their entry is not read); idle ones get no iterations
+            t = time.time()
+            statuses = batch.solve_any([params_for(p, want[p]) for p in range(K)], primal_weight,
+                                       resume=[p in running for p in range(K)])
+            stats.projection_time += time.time() - t
+            for p in new:
+                want[p] = False
+                running.add(p)
+            for p in sorted(running):
+                if statuses[p] == "RUNNING":
+                    continue
+                running.discard(p)
+                if advance(p):
+                    winner = p
+                    break
+    while not asynchronous:
         done = winner is not None or elapsed() >= time_limit
         if (stop(done) if stop is not None else done):
             break
@@ -633,42 +762,9 @@ def feasibility_pump_batched(milp: MILP, *, seeds=(101, 201), time_limit: float 
                 inner[p] += batch.results[p]["total_count"]
         stats.projection_time += time.time() - t
         for p, tr in enumerate(trajs):
-            tr.pdhg += inner[p]
-            if gaps[p] > gap_floor:
-                gaps[p] = max(gaps[p] * gap_decay, gap_floor)
-            xp = xs[p]
-            if is_integral(xp, int_idx, tol):
-                cand = _round_to_nearest(xp, milp)
-                if viol(cand) <= tol:
-                    tr.found, tr.x_found, tr.t_found = True, cand, elapsed()
-                    winner = p
-                    break
-            t = time.time()
-            x_round = round_guarded(tr.rounder, xp, tr.rng, tr.iterations)
-            stats.rounding_time += time.time() - t
-            candidate = tr.xt.copy()
-            if _differs(x_round, tr.xt, int_idx):
-                candidate[:] = x_round
-            else:
-                flips = int(tr.rng.integers(flip_parameter // 2, 3 * flip_parameter // 2 + 1))
-                _flip_farthest(candidate, xp, milp, flips)
-            h_candidate = _hash_integers(candidate, int_idx)
-            cycled = h_candidate in tr.seen
-            periodic = tr.since_restart >= restart_period
-            if cycled or periodic:
-                _perturb(candidate, xp, milp, tr.rng, tr.general, tr.is_general, tr.ladder,
-                         tr.iterations)
-                tr.perturbations += 1
-                tr.since_restart = 0
-                for _ in range(10):
-                    h = _hash_integers(candidate, int_idx)
-                    if not (h in tr.seen or h == tr.h_current):
-                        break
-                    _perturb(candidate, xp, milp, tr.rng, tr.general, tr.is_general, tr.ladder,
-                             tr.iterations)
-            tr.seen.add(tr.h_current)
-            tr.h_current = _hash_integers(candidate, int_idx) if (cycled or periodic) else h_candidate
-            tr.xt = candidate
+            if after_projection(p, xs[p], inner[p]):
+                winner = p
+                break
     best = trajs[winner] if winner is not None else trajs[0]
     stats.iterations = best.iterations
     stats.perturbations = best.perturbations

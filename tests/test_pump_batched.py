@@ -108,3 +108,52 @@ def test_gpu_batched_pump_mixed_finds_feasible(examples, name):
     res, trajs = feasibility_pump_batched(m, time_limit=120, seeds=(101, 201), precision="mixed")
     assert res.found and is_feasible(m, res.x)
     assert sum(t.found for t in trajs) == 1
+
+
+@pytest.mark.parametrize("name", ["p0201", "pk1", "markshare2"])
+def test_asynchronous_equals_lockstep_on_oracle(examples, oracle, name):
+    """The asynchronous driver with the oracle's solvers (every member's projection
+    ends within each call): the same trajectories, step for step, as lockstep."""
+    m = examples[name]
+    kw = dict(solvers=oracle.OracleSolvers(), time_limit=120, seeds=(101, 201),
+              batch_policy="always")
+    res_l, tr_l = feasibility_pump_batched(m, **kw)
+    res_a, tr_a = feasibility_pump_batched(m, asynchronous=True, **kw)
+    assert res_a.found == res_l.found
+    assert (res_a.iterations, res_a.pdhg_iterations, res_a.perturbations) == \
+        (res_l.iterations, res_l.pdhg_iterations, res_l.perturbations)
+    assert np.array_equal(res_a.x, res_l.x)
+    assert [(t.seed, t.found) for t in tr_a] == [(t.seed, t.found) for t in tr_l]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", EXAMPLES)
+def test_gpu_asynchronous_pump_trajectories_match_single_pumps(examples, name):
+    """FP64 batch on the GPU, asynchronous: each trajectory advances at its own pace
+    and takes exactly the steps of the single-trajectory pump with its seed; the
+    winner's result is that pump's result."""
+    m = examples[name]
+    singles = {s: feasibility_pump(m, time_limit=120, seed=s, precision="fp64",
+                                   batch_policy="always") for s in (101, 201)}
+    res, trajs = feasibility_pump_batched(m, time_limit=120, seeds=(101, 201), precision="fp64",
+                                          batch_policy="always", asynchronous=True)
+    assert res.found and is_feasible(m, res.x)
+    winners = [t for t in trajs if t.found]
+    assert len(winners) == 1
+    w = singles[winners[0].seed]
+    assert w.found
+    assert (res.iterations, res.pdhg_iterations, res.perturbations) == \
+        (w.iterations, w.pdhg_iterations, w.perturbations)
+    assert np.array_equal(res.x, w.x)
+    for t in trajs:  # the others stopped somewhere along their own single pump's path
+        assert t.iterations <= singles[t.seed].iterations or not singles[t.seed].found
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", EXAMPLES)
+def test_gpu_asynchronous_pump_mixed_finds_feasible(examples, name):
+    m = examples[name]
+    res, trajs = feasibility_pump_batched(m, time_limit=120, seeds=(101, 201), precision="mixed",
+                                          asynchronous=True)
+    assert res.found and is_feasible(m, res.x)
+    assert sum(t.found for t in trajs) == 1
