@@ -757,10 +757,10 @@ def pump_bench(args, world, rank, embed=False):
     coefficients plus 6 slacks in [0, 1000].  pump-p0201: binary covering models of
     p0201's shape (133 x 201, 1923 nonzeros).  Model seeds 1..32.  Arms: two
     trajectories (pump seeds 101 and 201) batched in one projector handle in mixed
-    precision, each advancing at its own pace (asynchronous); the same two in FP64;
-    the mixed pair in lockstep (every pump iteration waits for both projections); and
-    the plain FP64 single-trajectory pump (seed 101), the drop-in form of the
-    reference's GPU run.  Reported: p50/p90 of the wall time to the first feasible
+    precision, in lockstep (every pump iteration waits for both projections); the same
+    two in FP64; the mixed pair with each trajectory advancing at its own pace
+    (asynchronous); and the plain FP64 single-trajectory pump (seed 101), the drop-in
+    form of the reference's GPU run.  Reported: p50/p90 of the wall time to the first feasible
     point, root LP and handle construction included.  Ranks split the model seeds.
     """
     from pdfp_b200 import is_feasible, synthetic
@@ -768,7 +768,7 @@ def pump_bench(args, world, rank, embed=False):
     gen_name, config_text = PUMP_WORKLOADS[args.workload]
     gen = getattr(synthetic, gen_name)
     seeds = [s for s in range(1, 33) if (s - 1) % world == rank]
-    arms = {"mixed_batched": [], "fp64_batched": [], "mixed_batched_lockstep": [], "fp64_plain": []}
+    arms = {"mixed_batched": [], "fp64_batched": [], "mixed_batched_async": [], "fp64_plain": []}
     found = {k: 0 for k in arms}
     split = {k: [] for k in arms}  # (root LP, projections, rounding, pump iterations, PDHG iterations)
 
@@ -785,19 +785,18 @@ def pump_bench(args, world, rank, embed=False):
     for s in seeds:
         m = gen(s)
         t = time.perf_counter()
-        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="mixed", time_limit=60,
-                                        asynchronous=True)
+        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="mixed", time_limit=60)
         note("mixed_batched", r, time.perf_counter() - t)
         found["mixed_batched"] += int(r.found and is_feasible(m, r.x))
         t = time.perf_counter()
-        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="fp64", time_limit=60,
-                                        asynchronous=True)
+        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="fp64", time_limit=60)
         note("fp64_batched", r, time.perf_counter() - t)
         found["fp64_batched"] += int(r.found and is_feasible(m, r.x))
         t = time.perf_counter()
-        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="mixed", time_limit=60)
-        note("mixed_batched_lockstep", r, time.perf_counter() - t)
-        found["mixed_batched_lockstep"] += int(r.found and is_feasible(m, r.x))
+        r, _ = feasibility_pump_batched(m, seeds=(101, 201), precision="mixed", time_limit=60,
+                                        asynchronous=True)
+        note("mixed_batched_async", r, time.perf_counter() - t)
+        found["mixed_batched_async"] += int(r.found and is_feasible(m, r.x))
         t = time.perf_counter()
         r = feasibility_pump(m, seed=101, precision="fp64", time_limit=60)
         note("fp64_plain", r, time.perf_counter() - t)
