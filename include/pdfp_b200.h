@@ -290,6 +290,12 @@ PDFP_API int pdfp_get_tuning_reducers(const pdfp_handle* h, int32_t* out);
  * threshold l (and the partials pass's stage bytes, threads per role, stages
  * and blocks per segment); PDFP_SEG=0: off. */
 PDFP_API int pdfp_get_tuning_seg(const pdfp_handle* h, int32_t* out);
+/* How a window's minor steps run: *out = 0, two step launches per step replayed
+ * from a captured graph; 1, one cooperative launch of the per-block row passes
+ * (PDFP_MEDIUM=1); 2, one cooperative launch of the vec engine's warp items
+ * (PDFP_VEC_WINDOW=1, both FP32 sides on the vec engine without long-row
+ * pieces); 3, whole windows of each small member in one block's launch. */
+PDFP_API int pdfp_get_window_form(const pdfp_handle* h, int32_t* out);
 /* Every measurement the autotuner took: up to `cap` rows, ms[i] the mean
  * launch time, cfg[7i..7i+6] = {side (0: A', 1: A), stage bytes, gatherer
  * threads (0: flat engine; 32: vec engine, whose stage bytes are its nonzeros

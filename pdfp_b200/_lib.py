@@ -120,6 +120,7 @@ SIGNATURES = {
     "pdfp_get_tuning_blocks": (C.c_int, [vp, ip]),
     "pdfp_get_tuning_reducers": (C.c_int, [vp, ip]),
     "pdfp_get_tuning_seg": (C.c_int, [vp, ip]),
+    "pdfp_get_window_form": (C.c_int, [vp, ip]),
     "pdfp_profile_step": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                     dp, dp]),
     "pdfp_scale_problem": (C.c_int, [C.POINTER(Csr), dp, dp, dp, dp, dp, C.c_int32, C.c_double,

@@ -311,6 +311,13 @@ int pdfp_get_tuning_seg(const pdfp_handle* h, int32_t* out) {
     });
 }
 
+int pdfp_get_window_form(const pdfp_handle* h, int32_t* out) {
+    return guarded([&] {
+        if (!h || !h->proj || !out) throw pdfp::Error(PDFP_E_INVALID, "null argument");
+        *out = h->proj->window_form();
+    });
+}
+
 int pdfp_get_tuning_table(const pdfp_handle* h, float* ms, int32_t* cfg, int32_t cap,
                           int32_t* count) {
     return guarded([&] {

@@ -262,6 +262,7 @@ VecDev DeviceMatrix::make_vec(DeviceArena& ar, bool transpose, int lane_nnz) con
     const int32_t slots = build_vec_items(csr, transpose ? L.col_off : L.row_off, lane_nnz, items);
     VecDev v;
     v.n_items = static_cast<int32_t>(items.size());
+    v.n_slots = slots;
     v.rp = transpose ? rp_t : rp_a;
     v.ci = transpose ? ci_t : ci_a;
     v.items = ar.upload(items);

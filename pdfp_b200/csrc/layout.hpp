@@ -170,6 +170,7 @@ constexpr int kVecPiece = 1024;  // nonzeros per piece of a long row
 // Device view of one side of the matrix as vec-engine items.
 struct VecDev {
     int32_t n_items = 0;
+    int32_t n_slots = 0;  // long-row piece slots (0: no row longer than kVecPiece)
     const int32_t* rp = nullptr;
     const int32_t* ci = nullptr;
     const VecItem* items = nullptr;

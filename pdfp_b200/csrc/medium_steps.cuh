@@ -16,6 +16,7 @@
 #pragma once
 #include "common.cuh"
 #include "tiny_steps.cuh"
+#include "vec_spmv.cuh"
 
 namespace pdfp {
 
@@ -104,6 +105,28 @@ __global__ void __launch_bounds__(kMediumThreads)
         medium_pass(pop, rp_t, ci_t, col_off, K, ta, tb);  // the A'-side pass (primal update)
         if (!grid_barrier(bar, pop.err())) return;
         medium_pass(dop, rp_a, ci_a, row_off, K, aa, ab);  // the A-side pass (dual update)
+        if (!grid_barrier(bar, pop.err())) return;
+    }
+}
+
+// The vec engine's window: steps i0 .. i1-1 (minor) of every instance in one
+// cooperative launch of every resident block, the A'-side items (POp), a grid
+// barrier, the A-side items (DOp), a grid barrier, step after step.  Each warp
+// takes the same items in every step (warp w: items w, w + W, ...), so every row's
+// epilogue reads per-row vectors that only its own warp writes; the gathered
+// vectors, written by other blocks, are read from L2 (the Ops' L2-only policy).
+// The host uses it only for sides without long-row pieces, whose epilogues would
+// move between warps from step to step.
+template <class POp, class DOp>
+__global__ void __launch_bounds__(kVecThreads, 4)
+    vec_window_kernel(const VecDev ps, const VecDev ds, POp pop, DOp dop, GridBar bar,
+                      int32_t i0, int32_t i1) {
+    for (int32_t i = i0; i < i1; ++i) {
+        pop.k_offset = i;
+        dop.k_offset = i;
+        vec_pass<POp>(ps, pop);  // the A'-side pass (primal update)
+        if (!grid_barrier(bar, pop.err())) return;
+        vec_pass<DOp>(ds, dop);  // the A-side pass (dual update)
         if (!grid_barrier(bar, pop.err())) return;
     }
 }

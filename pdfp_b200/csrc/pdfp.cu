@@ -919,6 +919,28 @@ Projector::Projector(const std::vector<ProblemData>& probs, int precision) : pre
         prepare_side(p64_, true, false);
         prepare_side(d64_, false, false);
     }
+    // PDFP_VEC_WINDOW=1: when both sides of the FP32 steps run on the vec engine and
+    // neither has long-row pieces, a window's minor steps run in one cooperative launch
+    // (vec_window_kernel) instead of two launches per step
+    {
+        const char* vw = std::getenv("PDFP_VEC_WINDOW");
+        vecwin_ = vw && vw[0] == '1' && precision_ == PDFP_MIXED && !tiny_ && p32_.engine == 2 &&
+                  d32_.engine == 2 && p32_.vec.n_slots == 0 && d32_.vec.n_slots == 0;
+        if (vecwin_) {
+            int coop = 0, dev = 0, per_sm = 0;
+            PDFP_CK(cudaGetDevice(&dev));
+            PDFP_CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+            PDFP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, vec_window_kernel<PrimalOp<float, false, kFlatThreads>, DualOp<float, false, kFlatThreads>>,
+                kVecThreads, 0));
+            if (!coop || per_sm < 1) {
+                vecwin_ = false;
+            } else {
+                vecwin_grid_ = per_sm * num_sms_;
+                if (!gbar_) gbar_ = ar_.alloc<unsigned>(4);
+            }
+        }
+    }
 }
 
 template <>
@@ -1526,6 +1548,27 @@ void Projector::launch_medium_steps(int i0, int i1) {
                                static_cast<int32_t>(i1)));
 }
 
+void Projector::launch_vec_window(int i0, int i1) {
+    using POp = PrimalOp<float, false, kFlatThreads>;
+    using DOp = DualOp<float, false, kFlatThreads>;
+    // gathers read L2 (policy 1): the gathered vectors were written by other blocks
+    const POp pop{v32_, st_, 0, MODE_FP32, err_, 1};
+    const DOp dop{v32_, st_, M_.row_off, M_.n_eq, 0, MODE_FP32, err_, 1};
+    const GridBar bar{gbar_, gbar_ + 1, gbar_ + 2};
+    PDFP_CK(cudaMemsetAsync(gbar_, 0, sizeof(unsigned) * 4, stream_));  // count, generation, abort
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(vecwin_grid_));
+    cfg.blockDim = dim3(kVecThreads);
+    cfg.stream = stream_;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    PDFP_CK(cudaLaunchKernelEx(&cfg, vec_window_kernel<POp, DOp>, p32_.vec, d32_.vec, pop, dop, bar,
+                               static_cast<int32_t>(i0), static_cast<int32_t>(i1)));
+}
+
 // Timing mode's plan for a window of `freq` steps: the RUN, minor steps
 // [run_a, run_b) in the middle half of steps 2 .. freq-1, is bracketed by two events
 // and nothing else, so it times the average step as the other windows run it; up to
@@ -1591,6 +1634,13 @@ void Projector::record_window(int freq, bool with32, bool with64) {
             // steps 2 .. freq-1 in one launch per precision
             if (with32) launch_tiny_steps<float>(2, freq);
             if (with64) launch_tiny_steps<double>(2, freq);
+            after_step = false;
+            i = freq - 1;
+            continue;
+        }
+        if (vecwin_ && with32 && !with64 && !sample && i == 2 && freq > 2) {
+            // steps 2 .. freq-1 of the FP32 steps on the vec engine in one cooperative launch
+            launch_vec_window(2, freq);
             after_step = false;
             i = freq - 1;
             continue;

@@ -68,6 +68,9 @@ class Projector {
     // The A-side step of the FP32 steps with its long rows by column segment:
     // {segments, long-row threshold}, {0, 0} when it has none.
     void tuning_seg(int32_t* out) const;
+    // 0: per-step launches (graph), 1: cooperative row passes, 2: cooperative vec
+    // window, 3: whole windows per small member in one launch
+    int32_t window_form() const { return tiny_ ? 3 : vecwin_ ? 2 : medium_ ? 1 : 0; }
     // Every autotuner measurement: ms[i] and cfg[7i..7i+6] = {side (0: A', 1: A),
     // stage bytes, gatherer threads, gather policy, stages, blocks per SM cap,
     // reducer threads}; side 2: the A side with its long rows by column segment,
@@ -200,6 +203,9 @@ class Projector {
     bool medium_ = false;  // a mid-sized handle: the minor steps in one cooperative launch
     int32_t *part_t_ = nullptr, *part_a_ = nullptr;  // each block's rows of A' and of A
     unsigned* gbar_ = nullptr;                          // the grid barrier's words
+    bool vecwin_ = false;  // FP32 minor steps of a window in one cooperative vec launch
+    int vecwin_grid_ = 0;  // its blocks (all resident)
+    void launch_vec_window(int i0, int i1);
     cudaEvent_t tev_[2 + 3 * kSplitSteps] = {};  // timing mode: the run's two, then 3 per split step
     cudaEvent_t sev_[2] = {nullptr, nullptr};              // whole solve
 };

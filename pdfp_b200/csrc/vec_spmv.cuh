@@ -121,8 +121,9 @@ __device__ __forceinline__ void vec_piece(const VecDev& s, const Op& op, const V
     }
 }
 
+// One pass over a side's items: warp w of the grid takes items w, w + W, ...
 template <class Op>
-__global__ void __launch_bounds__(kVecThreads, 4) vec_spmv_kernel(const VecDev s, const Op op) {
+__device__ __forceinline__ void vec_pass(const VecDev& s, const Op& op) {
     using VT = typename Op::VT;
     static_assert(Op::NV == 1 && Op::NP == 0, "the vec engine runs the step passes");
     constexpr int NVEC = Op::NVEC;
@@ -130,8 +131,8 @@ __global__ void __launch_bounds__(kVecThreads, 4) vec_spmv_kernel(const VecDev s
 #pragma unroll
     for (int k = 0; k < NVEC; ++k) sv[k] = op.staged(k);
     const int lane = threadIdx.x & 31;
-    const int32_t w0 = static_cast<int32_t>((blockIdx.x * kVecThreads + threadIdx.x) >> 5);
-    const int32_t nw = static_cast<int32_t>((gridDim.x * kVecThreads) >> 5);
+    const int32_t w0 = static_cast<int32_t>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int32_t nw = static_cast<int32_t>((gridDim.x * blockDim.x) >> 5);
     for (int32_t it = w0; it < s.n_items; it += nw) {
         const VecItem m = s.items[it];
         if (!op.active(m.inst)) continue;
@@ -141,6 +142,11 @@ __global__ void __launch_bounds__(kVecThreads, 4) vec_spmv_kernel(const VecDev s
         else
             vec_rows<Op>(s, op, m, tp, sv, lane);
     }
+}
+
+template <class Op>
+__global__ void __launch_bounds__(kVecThreads, 4) vec_spmv_kernel(const VecDev s, const Op op) {
+    vec_pass<Op>(s, op);
 }
 
 }  // namespace pdfp

@@ -101,3 +101,33 @@ def test_vec_bad_pins(zipf, monkeypatch, pin, msg):
     monkeypatch.setenv("PDFP_TUNING", pin)
     with pytest.raises(Exception, match=msg):
         solve(zipf, "mixed")
+
+
+def window_form(s):
+    out = gpu.C.c_int32()
+    gpu.L.check(gpu.L.lib().pdfp_get_window_form(s._h, gpu.C.byref(out)))
+    return out.value
+
+
+@pytest.mark.parametrize("tol", [1e-4, 1e-5])
+def test_vec_window_equals_per_step_launches(oracle, monkeypatch, tol):
+    """PDFP_VEC_WINDOW=1: a window's minor steps in one cooperative launch of the vec
+    engine (a grid barrier between the passes) take the same steps as two vec
+    launches per step, bit for bit (every row's arithmetic is the same; each row's
+    epilogue stays on one warp), on the 20k x 50k general-integer model."""
+    milp, _, xt = synthetic.general_integer(1)
+    sc, is_eq, is_int, w = oracle.projector_inputs(milp)
+    prm = SolverParameters(eps_optimal_relative=tol, eps_feasible_relative=tol)
+    monkeypatch.setenv("PDFP_STEP_ENGINE", "vec")
+    out = {}
+    for vw in ("0", "1"):
+        monkeypatch.setenv("PDFP_VEC_WINDOW", vw)
+        s = gpu.PDFPState(sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w, precision="mixed")
+        assert window_form(s) == (2 if vw == "1" else 0)
+        s.set_target(xt / sc.D_c)
+        st = s.solve(prm, 1.0)
+        out[vw] = (st, s.total_count, s.pdhg_x, s.get("pdhg_z"), s.get("current_y"))
+    assert out["0"][0] == out["1"][0] == "OPTIMAL"
+    assert out["0"][1] == out["1"][1]
+    for a, b in zip(out["0"][2:], out["1"][2:]):
+        assert np.array_equal(a, b)
