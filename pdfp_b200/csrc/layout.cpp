@@ -74,11 +74,11 @@ void build_tiling(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
 }
 
 int32_t build_vec_items(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
-                        int lane_nnz, std::vector<VecItem>& items) {
+                        int lane_nnz, std::vector<VecItem>& items, int groups) {
     items.clear();
     const int K = static_cast<int>(inst_row_off.size()) - 1;
     const std::vector<int32_t>& rp = csr.rp;
-    const int rpg = std::max(1, 8 / std::max(1, lane_nnz));
+    const int rpg = groups > 0 ? groups : std::max(1, 8 / std::max(1, lane_nnz));
     auto lanes_log2 = [&](int64_t len) {
         int lg = 0;
         while (lg < 5 && (int64_t(1) << lg) * lane_nnz < len) ++lg;

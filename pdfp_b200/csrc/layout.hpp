@@ -181,11 +181,12 @@ struct VecDev {
 // Items of one side: rows longer than kVecPiece are cut into pieces; the other
 // rows get the lanes per row that give each lane about `lane_nnz` nonzeros (a
 // power of two up to 32), and runs of rows with equal lanes are cut into items
-// of (32 / lanes) x max(1, 8 / lane_nnz) rows, fewer where the item would hold
-// more than 2048 nonzeros.  Items are ordered longest-first: pieces, then by
-// decreasing lanes per row, each group in row order.  Returns the slot count.
+// of (32 / lanes) x `groups` rows (groups <= 0: max(1, 8 / lane_nnz)), fewer where
+// the item would hold more than 2048 nonzeros.  Items are ordered longest-first:
+// pieces, then by decreasing lanes per row, each group in row order.  Returns the
+// slot count.
 int32_t build_vec_items(const HostCsr& csr, const std::vector<int32_t>& inst_row_off,
-                        int lane_nnz, std::vector<VecItem>& items);
+                        int lane_nnz, std::vector<VecItem>& items, int groups = 0);
 
 // The long rows of A by column segment (seg_spmv.cuh).  The packed columns are cut
 // into nseg segments of seg_len (a multiple of 4; the last segments may be short

@@ -101,8 +101,21 @@ struct PrimalOp {
     __device__ const T* gather_src() const { return v.cz; }
     __device__ void row(int32_t j, int32_t rr, int inst, const TileP& p, const T* const* sv,
                         const T (&s)[1], double*) const {
-        const T cx = sv[0][rr], ix = sv[1][rr], cy = sv[2][rr], iy = sv[3][rr];
-        const T lb = sv[4][rr], ub = sv[5][rr], xt = sv[6][rr], w = sv[7][rr];
+        T pv[NVEC];
+#pragma unroll
+        for (int q = 0; q < NVEC; ++q) pv[q] = sv[q][rr];
+        row_vals(j, p, pv, s);
+    }
+    // Column j's per-column inputs from global memory, in staged() order, cached in L2
+    // only: L1 stays for the gathered z entries that long rows share.
+    __device__ void load_row(int32_t j, T (&pv)[NVEC]) const {
+#pragma unroll
+        for (int q = 0; q < NVEC; ++q) pv[q] = __ldcg(staged(q) + j);
+    }
+    // The epilogue on column j's inputs pv (staged() order) and its sum s = (A'z)_j.
+    __device__ void row_vals(int32_t j, const TileP& p, const T (&pv)[NVEC], const T (&s)[1]) const {
+        const T cx = pv[0], ix = pv[1], cy = pv[2], iy = pv[3];
+        const T lb = pv[4], ub = pv[5], xt = pv[6], w = pv[7];
         // primal_step!  (src/pdfp.jl:124-129)
         const T t = sub_rn(cx, mul_rn(p.tau, sub_rn(s[0], cy)));
         const T xh = jl_clamp(t, lb, ub);
@@ -159,7 +172,19 @@ struct DualOp {
     __device__ const T* gather_src() const { return v.rx; }
     __device__ void row(int32_t i, int32_t rr, int inst, const TileP& t, const T* const* sv,
                         const T (&s)[1], double*) const {
-        const T cz = sv[0][rr], iz = sv[1][rr], b = sv[2][rr];
+        T pv[NVEC];
+#pragma unroll
+        for (int q = 0; q < NVEC; ++q) pv[q] = sv[q][rr];
+        row_vals(i, t, pv, s);
+    }
+    // Row i's per-row inputs from global memory, in staged() order.
+    __device__ void load_row(int32_t i, T (&pv)[NVEC]) const {
+#pragma unroll
+        for (int q = 0; q < NVEC; ++q) pv[q] = staged(q)[i];
+    }
+    // The epilogue on row i's inputs pv (staged() order) and its sum s = (A x_bar)_i.
+    __device__ void row_vals(int32_t i, const TileP& t, const T (&pv)[NVEC], const T (&s)[1]) const {
+        const T cz = pv[0], iz = pv[1], b = pv[2];
         // dual_z_step!  (src/pdfp.jl:150-154)
         const T raw = add_rn(cz, mul_rn(t.p.sigma, sub_rn(s[0], b)));
         const T zh = i < t.eq_end ? raw : jl_max(raw, T(0));

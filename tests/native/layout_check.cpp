@@ -57,9 +57,10 @@ static int check_tiling(const HostCsr& csr, const std::vector<int32_t>& off, con
 
 // Vec-engine items (build_vec_items): every row once, in a multi-row item of its
 // instance or as pieces that cover its nonzeros in order; lanes and sizes in range.
-static int check_vec(const HostCsr& csr, const std::vector<int32_t>& off, int lane_nnz) {
+static int check_vec(const HostCsr& csr, const std::vector<int32_t>& off, int lane_nnz,
+                     int groups = 0) {
     std::vector<VecItem> items;
-    const int32_t slots = build_vec_items(csr, off, lane_nnz, items);
+    const int32_t slots = build_vec_items(csr, off, lane_nnz, items, groups);
     const int K = static_cast<int>(off.size()) - 1;
     std::vector<int> seen(csr.rows, 0);
     std::vector<int32_t> next_k(csr.rows, -1);
@@ -266,12 +267,13 @@ extern "C" int layout_check(int K, const int32_t* ms, const int32_t* ns, const i
             if (rc) return 300 + rc;
         }
     // the vec engine's items
-    for (int lane : {1, 2, 4, 8}) {
-        int rc = check_vec(L.At, L.col_off, lane);
-        if (rc) return 400 + rc;
-        rc = check_vec(L.A, L.row_off, lane);
-        if (rc) return 500 + rc;
-    }
+    for (int lane : {1, 2, 4, 8})
+        for (int groups : {0, 32 / lane}) {  // the default rows per item and four times them
+            int rc = check_vec(L.At, L.col_off, lane, groups);
+            if (rc) return 400 + rc;
+            rc = check_vec(L.A, L.row_off, lane, groups);
+            if (rc) return 500 + rc;
+        }
     // segmented long rows: small stages, so that pairs span several tiles and long
     // pairs several chunks
     stats[2] = 0;
