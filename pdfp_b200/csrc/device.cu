@@ -260,11 +260,14 @@ VecDev DeviceMatrix::make_vec(DeviceArena& ar, bool transpose, int lane_nnz, int
     const HostCsr& csr = transpose ? L.At : L.A;
     const std::vector<int32_t>& off = transpose ? L.col_off : L.row_off;
     std::vector<VecItem> items;
-    // four times the default rows per item (fewer items to fetch per warp) while that
-    // still leaves at least min_items items for the warps of the grid
-    const int groups = std::max(1, 32 / std::max(1, lane_nnz));
-    int32_t slots = build_vec_items(csr, off, lane_nnz, items, groups);
-    if (static_cast<int64_t>(items.size()) < min_items) slots = build_vec_items(csr, off, lane_nnz, items);
+    int32_t slots = 0;
+    if (min_items > 0) {
+        // four times the default rows per item (fewer items to fetch per warp) while
+        // that still leaves at least min_items items for the warps of the grid
+        slots = build_vec_items(csr, off, lane_nnz, items, std::max(1, 32 / std::max(1, lane_nnz)));
+        if (static_cast<int64_t>(items.size()) < min_items) items.clear();
+    }
+    if (items.empty()) slots = build_vec_items(csr, off, lane_nnz, items);
     VecDev v;
     v.n_items = static_cast<int32_t>(items.size());
     v.n_slots = slots;

@@ -174,7 +174,7 @@ class DeviceMatrix {
                        const std::vector<uint8_t>* skip = nullptr) const;
     // Build and upload the vec engine's items of A (transpose = false) or A'
     // (build_vec_items), with zeroed piece slots and counters; items of four times the
-    // default rows when that still gives at least `min_items` items.
+    // default rows when min_items > 0 and that still gives at least min_items items.
     VecDev make_vec(DeviceArena& ar, bool transpose, int lane_nnz, int64_t min_items) const;
     // Build and upload A's long rows by column segment (build_seg) and a tiling of
     // their (segment, long row) pairs in stage geometry g, interleaved one block per

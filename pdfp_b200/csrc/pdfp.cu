@@ -1004,9 +1004,11 @@ void Projector::prepare_side(StepSide& s, bool primal, bool f32) {
     if (s.engine != 0) s.seg_nseg = 0;  // segmented long rows: tile engine only
     if (s.engine == 2) {
         if (!f32) throw Error(E_INVALID, "internal: the vec engine runs the FP32 steps only");
-        // at least two items per warp of a full grid of the vec kernel
+        // The A' side (short, even rows on the zipf-lp matrix: 68 us against 72 us a
+        // launch) takes larger items while they leave at least two per warp of a full
+        // grid; on the A side (Zipf-skewed rows) larger items measured slower.
         s.vec = M_.make_vec(ar_, primal, s.lane_nnz,
-                            int64_t(2) * num_sms_ * kVecMinBlocks * (kVecThreads / 32));
+                            primal ? int64_t(2) * num_sms_ * kVecMinBlocks * (kVecThreads / 32) : 0);
         s.stage_bytes = s.lane_nnz;
         s.nt = 32;
         s.half_red = false;
