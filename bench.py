@@ -674,6 +674,12 @@ def batch_uneven(args, world, rank, local, embed=False):
         bt = gpu.PDFPBatch(probs, precision=precision)
         for p in range(len(probs)):
             bt.set_col_scale(p, scs[p].D_c)
+        tun = (gpu.C.c_int32 * 8)()
+        gpu.L.check(gpu.L.lib().pdfp_get_tuning(bt._h, tun))
+        engine = {0: "flat", 32: "vec"}
+        tuning = {"a_t_engine": engine.get(tun[1], "tile"), "a_t_stage_bytes": tun[0],
+                  "a_t_threads": tun[1], "a_engine": engine.get(tun[4], "tile"),
+                  "a_stage_bytes": tun[3], "a_threads": tun[4]}
         x_outs = [gpu.pinned_zeros(n) for n in ns]
         log(f"[bench] {precision} batch handle built in {time.time() - t:.1f}s")
         per = []
@@ -703,7 +709,7 @@ def batch_uneven(args, world, rank, local, embed=False):
         iters = allreduce(world, sum(p["iters"] for p in timed), "sum")
         byts = allreduce(world, sum(p["bytes"] for p in timed), "sum")
         res[precision] = {"dev_s": dev_s, "wall_s": wall_s, "iters": iters, "bytes": byts,
-                          "clocks": clk.summary(), "steps": timed}
+                          "clocks": clk.summary(), "steps": timed, "tuning": tuning}
         bt.close()
     if rank != 0:
         return
@@ -718,7 +724,7 @@ def batch_uneven(args, world, rank, local, embed=False):
                        "[1000, 200000], m = 0.6 n, 10-40 nnz/row, one batch handle; eps_opt 1e-4, "
                        "eps_feas 1e-5 per instance", "instances": len(probs), "sum_n": sum(ns),
                        "sum_m": sum(ms), "sum_nnz": sum(nnz), "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2"},
+                       "l2": "inputs larger than L2", "tuning": mx["tuning"]},
             "hbm_gbs": round(mx["bytes"] / mx["dev_s"] / world / 1e9, 1),
             "hbm_frac": round(mx["bytes"] / mx["dev_s"] / world / 1e9 / peak, 4),
             "peak_kind": peak_kind,
