@@ -415,6 +415,8 @@ def main():
         extras["batch_uneven"] = batch_uneven(sub, world, rank, local, embed=True)
         sub.workload = "pump-markshare"
         extras["pump_markshare"] = pump_bench(sub, world, rank, embed=True)
+        if rank == 0:
+            extras["p0201_published"] = p0201_published()
 
     refform_line = None
     if not args.no_refform:
@@ -755,6 +757,57 @@ PUMP_WORKLOADS = {
                    "coefficients U{1..5}, b = 1 + floor(0.3 rowsum), c U{1..100}, model seeds "
                    "1..32, pump seeds 101 and 201 (flip_parameter 20, restart_period 100)"),
 }
+
+
+# The one run the reference publishes (README.md:36-48): p0201 on an NVIDIA H100 80GB
+# HBM3, root LP "OPTIMAL after 600 iterations, 0.03 s", pump "FEASIBLE after 5
+# iterations, 0.12 s", "root LP 0.03 s, projections 0.09 s, rounding 0.00 s".
+P0201_PUBLISHED_S = {"total": 0.12, "root_lp": 0.03, "projection": 0.09, "root_lp_iterations": 600,
+                     "pump_iterations": 5}
+
+
+def p0201_published(runs: int = 12, warmup: int = 2):
+    """The reference's published example run, on the real p0201 instance (the committed
+    fixture tests/golden/p0201.npz, made from the reference's examples/p0201.mps.gz):
+    the full pump with the drop-in FP64 solvers and the reference's default parameters,
+    `runs` pump seeds after `warmup` untimed runs.  Wall-clock times as the reference's
+    log reports them; its later pump iterations follow Julia's MersenneTwister draws,
+    which this pump does not reproduce, so the iteration counts differ by seed."""
+    import scipy.sparse as sp
+    from pdfp_b200.milp import MILP
+    from pdfp_b200.pump import feasibility_pump
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "p0201.npz")
+    d = np.load(path)
+    A = sp.csr_matrix((d["data"], d["indices"], d["indptr"]), shape=tuple(d["shape"]))
+    milp = MILP(d["c"], float(d["c0"]), A, d["b"], ["eq" if e else "le" for e in d["is_eq"]],
+                d["l"], d["u"], d["int_idx"], name=str(d["name"]))
+    rows = []
+    for seed in range(1, warmup + runs + 1):
+        r = feasibility_pump(milp, time_limit=60.0, seed=seed, precision="fp64")
+        if seed > warmup:
+            rows.append(r)
+    med = lambda xs: statistics.median(xs)  # noqa: E731
+    ours = {"total_s": round(med([r.time for r in rows]), 5),
+            "root_lp_s": round(med([r.root_lp_time for r in rows]), 5),
+            "projection_s": round(med([r.projection_time for r in rows]), 5),
+            "rounding_s": round(med([r.rounding_time for r in rows]), 5),
+            "found": sum(r.found for r in rows), "runs": len(rows),
+            "pump_iterations": sorted(r.iterations for r in rows),
+            "root_lp_status": sorted(set(r.root_lp_status for r in rows))}
+    log(f"[bench] p0201 (published run): {ours}")
+    return {"workload": "p0201 (the reference's published example: 133 x 201, 1923 nonzeros), "
+                        "full pump, FP64 drop-in form, reference defaults, pump seeds "
+                        f"{warmup + 1}..{warmup + runs}",
+            "ours_median": ours,
+            "published_h100": {"total_s": P0201_PUBLISHED_S["total"],
+                               "root_lp_s": P0201_PUBLISHED_S["root_lp"],
+                               "projection_s": P0201_PUBLISHED_S["projection"],
+                               "root_lp_iterations": P0201_PUBLISHED_S["root_lp_iterations"],
+                               "pump_iterations": P0201_PUBLISHED_S["pump_iterations"],
+                               "source": "reference README.md:36-48 (NVIDIA H100 80GB HBM3)"},
+            "time_ratio_published_over_ours": {
+                "total": round(P0201_PUBLISHED_S["total"] / ours["total_s"], 1),
+                "root_lp": round(P0201_PUBLISHED_S["root_lp"] / ours["root_lp_s"], 1)}}
 
 
 def pump_bench(args, world, rank, embed=False):
