@@ -83,7 +83,7 @@ __device__ __forceinline__ void medium_pass(const Op& op, const int32_t* __restr
         if (!op.active(p)) continue;  // block-uniform
         const int32_t a = off[p] > ra ? off[p] : ra;
         const int32_t b = off[p + 1] < rb ? off[p + 1] : rb;
-        if (a < b) tiny_pass<Op, kMediumThreads>(op, rp, ci, a, b, p);
+        if (a < b) tiny_pass<Op, kMediumThreads, 4>(op, rp, ci, a, b, p);  // 4: its register budget
     }
 }
 

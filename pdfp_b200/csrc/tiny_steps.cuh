@@ -17,12 +17,39 @@ namespace pdfp {
 
 constexpr int kTinyThreads = 256;
 
-template <class Op, int NTH = kTinyThreads>
+// A lane's share of one row's sum: its nonzeros k0, k0 + G, ... below `end`, U at a
+// time, added to s in storage order.  All U index, value and gather loads of a group
+// are issued before its first product is added.
+template <int U, class Op>
+__device__ __forceinline__ void tiny_row_sum(const Op& op, const int32_t* __restrict__ ci,
+                                             const typename Op::MT* vals, int32_t k0, int32_t end,
+                                             int G, typename Op::AT& s) {
+    using AT = typename Op::AT;
+    using GT = typename Op::GT;
+    for (; k0 < end; k0 += U * G) {
+        int32_t c[U];
+        AT a[U];
+        GT g[U][1];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t kk = k0 + u * G;
+            c[u] = kk < end ? ci[kk] : 0;
+            a[u] = kk < end ? static_cast<AT>(vals[kk]) : AT(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u * G < end) op.gather(c[u], g[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u * G < end) s = add_rn(s, mul_rn(a[u], static_cast<AT>(g[u][0])));
+    }
+}
+
+template <class Op, int NTH = kTinyThreads, int UONE = 8>
 __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restrict__ rp,
                                           const int32_t* __restrict__ ci, int32_t r0, int32_t r1,
                                           int inst) {
     using AT = typename Op::AT;
-    using GT = typename Op::GT;
     using VT = typename Op::VT;
     constexpr int NVEC = Op::NVEC;
     const VT* sv[NVEC];
@@ -41,27 +68,14 @@ __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restric
         AT s = AT(0);
         if (rr < R) {
             const int32_t row = r0 + rr;
-            const int32_t end = rp[row + 1];
-            // four of the lane's nonzeros at a time: their index, value and gather
-            // loads are all issued before the first product is added (same order)
-            constexpr int U = 4;
-            for (int32_t k0 = rp[row] + lane; k0 < end; k0 += U * G) {
-                int32_t c[U];
-                AT a[U];
-                GT g[U][1];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int32_t kk = k0 + u * G;
-                    c[u] = kk < end ? ci[kk] : 0;
-                    a[u] = kk < end ? static_cast<AT>(vals[kk]) : AT(0);
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (k0 + u * G < end) op.gather(c[u], g[u]);
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (k0 + u * G < end) s = add_rn(s, mul_rn(a[u], static_cast<AT>(g[u][0])));
-            }
+            // a row summed by one thread is a chain of dependent adds: UONE (eight)
+            // loads in flight per group let it wait for memory once per eight
+            // nonzeros (rows of 50-70 nonzeros on the reference's examples); rows
+            // shared by G > 1 lanes are short per lane and take four
+            if (G == 1)
+                tiny_row_sum<UONE>(op, ci, vals, rp[row], rp[row + 1], 1, s);
+            else
+                tiny_row_sum<4>(op, ci, vals, rp[row] + lane, rp[row + 1], G, s);
         }
         for (int o = G >> 1; o > 0; o >>= 1) s = add_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
         if (rr < R && lane == 0) {
@@ -76,6 +90,35 @@ __device__ __forceinline__ void tiny_pass(const Op& op, const int32_t* __restric
 // (rowsum[q * R + rr]), then the Op's per-row terms accumulate into acc with row rr on
 // thread rr % NTH -- the tile engine epilogue's assignment -- so that the block sum
 // that follows adds them in the same order as a one-tile evaluation launch.
+// The NV sums of an evaluation Op over a lane's share of one row (as tiny_row_sum).
+template <int U, class Op>
+__device__ __forceinline__ void tiny_row_sums(const Op& op, const int32_t* __restrict__ ci,
+                                              const typename Op::MT* vals, int32_t k0, int32_t end,
+                                              int G, typename Op::AT (&s)[Op::NV]) {
+    using AT = typename Op::AT;
+    using GT = typename Op::GT;
+    constexpr int NV = Op::NV;
+    for (; k0 < end; k0 += U * G) {
+        int32_t c[U];
+        AT a[U];
+        GT g[U][NV];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t kk = k0 + u * G;
+            c[u] = kk < end ? ci[kk] : 0;
+            a[u] = kk < end ? static_cast<AT>(vals[kk]) : AT(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u * G < end) op.gather(c[u], g[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u * G < end)
+#pragma unroll
+                for (int q = 0; q < NV; ++q) s[q] = add_rn(s[q], mul_rn(a[u], static_cast<AT>(g[u][q])));
+    }
+}
+
 template <class Op, int NTH = kTinyThreads>
 __device__ __forceinline__ void tiny_eval_pass(const Op& op, const int32_t* __restrict__ rp,
                                                const int32_t* __restrict__ ci, int32_t r0,
@@ -97,13 +140,12 @@ __device__ __forceinline__ void tiny_eval_pass(const Op& op, const int32_t* __re
         for (int q = 0; q < NV; ++q) s[q] = AT(0);
         if (rr < R) {
             const int32_t row = r0 + rr;
-            for (int32_t k = rp[row] + lane; k < rp[row + 1]; k += G) {
-                GT g[NV];
-                op.gather(ci[k], g);
-                const AT a = static_cast<AT>(vals[k]);
-#pragma unroll
-                for (int q = 0; q < NV; ++q) s[q] = add_rn(s[q], mul_rn(a, static_cast<AT>(g[q])));
-            }
+            // one lane per row: four of its nonzeros in flight at a time; several lanes
+            // per row: one at a time (added in storage order either way)
+            if (G == 1)
+                tiny_row_sums<4>(op, ci, vals, rp[row], rp[row + 1], 1, s);
+            else
+                tiny_row_sums<1>(op, ci, vals, rp[row] + lane, rp[row + 1], G, s);
         }
         for (int o = G >> 1; o > 0; o >>= 1)
 #pragma unroll
