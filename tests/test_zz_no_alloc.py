@@ -8,7 +8,8 @@ device array of the library instead.  The test allocates the caller's own
 device arrays (the matrix) with torch, calls the entry point through the C
 ABI twice in a row, and checks both results against the allocating entry
 point pdfp_estimate_max_singular_value (same algorithm, start vector and
-summation order; estimates within 1e-10 relative, equal iteration counts).
+summation order; estimates within 1e-10 relative, equal iteration counts),
+and two of the cases against the CPU oracle's power iteration as well.
 
 It also checks that a call made after the first on a device changes neither
 the device's free memory nor torch's allocator, runs a case near the scratch
@@ -84,6 +85,20 @@ def test_noalloc_matches_allocating_entry_point_twice(idx):
         s, it = _noalloc(A)
         assert s == pytest.approx(ref, rel=1e-10)
         assert it == ref_it
+
+
+@pytest.mark.parametrize("idx", [0, 2])
+def test_noalloc_matches_the_oracle(idx):
+    """Pinned to the oracle's restatement of estimate_max_singular_value
+    (src/preconditioner.jl:108-125) directly, not only through the allocating
+    entry point: the same estimate to 1e-10 relative (the tolerance used against the
+    allocating entry point) and the same iteration count."""
+    from oracle import oracle as O
+    A = _matrices()[idx]
+    so, io = O.estimate_max_singular_value(sp.csr_matrix(A))
+    s, it = _noalloc(A)
+    assert s == pytest.approx(so, rel=1e-10)
+    assert it == io
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
