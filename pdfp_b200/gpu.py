@@ -276,6 +276,12 @@ class PDFPBatch:
         self.results = [r.as_dict() for r in rs]
         return [r["status"] for r in self.results]
 
+    def tuning(self):
+        """The step kernels' configuration (pdfp_get_tuning), as PDFPState.tuning reports it."""
+        out = (C.c_int32 * 8)()
+        L.check(L.lib().pdfp_get_tuning(self._h, out))
+        return list(out)
+
     def solve_any(self, params, primal_weights, resume=None):
         """pdfp_solve_batch_any: solve until at least one running member stops.
 

@@ -131,3 +131,39 @@ def test_vec_window_equals_per_step_launches(oracle, monkeypatch, tol):
     assert out["0"][1] == out["1"][1]
     for a, b in zip(out["0"][2:], out["1"][2:]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("lane_nnz", [2, 8])
+def test_vec_batch_members_equal_single_handles(oracle, monkeypatch, lane_nnz):
+    """A batch handle on the vec engine (both sides pinned; PDFP_TINY=0 so that the step
+    kernels run instead of the one-block path): five uneven covering/packing members,
+    which stop at different iterations.  Each member takes exactly the steps of its own
+    single handle: the same status, iteration count and iterates bit for bit.  A row's
+    sum does not depend on which work item holds it (nor on the larger items the A'
+    side takes when the handle has enough of them), a warp's step parameters are
+    recomputed when its item belongs to another member, and the items of members that
+    have stopped are skipped."""
+    monkeypatch.setenv("PDFP_TUNING", f"{lane_nnz},32,0,{lane_nnz},32,1")
+    monkeypatch.setenv("PDFP_TINY", "0")
+    models = synthetic.covering_packing_batch(seed=7, k=5, n_min=2000, n_max=20000)
+    rng = np.random.default_rng(21)
+    probs, targets, dcs = [], [], []
+    for m in models:
+        sc, is_eq, is_int, w = oracle.projector_inputs(m)
+        probs.append((sc.A, sc.con_ub, is_eq, is_int, sc.var_lb, sc.var_ub, w))
+        targets.append(np.round(rng.random(len(m.c))) / sc.D_c)
+        dcs.append(sc.D_c)
+    prm = SolverParameters(eps_optimal_relative=1e-4, eps_feasible_relative=1e-5)
+    b = gpu.PDFPBatch(probs, precision="mixed")
+    assert b.tuning()[1] == 32 and b.tuning()[4] == 32  # both sides on the vec engine
+    for p, xt in enumerate(targets):
+        b.set_target(p, xt)
+    st = b.solve(prm, 1.0)
+    counts = [r["total_count"] for r in b.results]
+    assert len(set(counts)) > 1  # members stop at different iterations
+    for p, pr in enumerate(probs):
+        s = gpu.PDFPState(*pr, precision="mixed")
+        s.set_target(targets[p])
+        assert s.solve(prm, 1.0) == st[p], p
+        assert s.total_count == counts[p], p
+        assert np.array_equal(s.pdhg_x, b.get(p, "pdhg_x")), p
