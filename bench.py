@@ -444,7 +444,7 @@ def main():
         default = (args.workload, args.m, args.n, args.nnz) == ("zipf-lp", 1_000_000, 2_000_000,
                                                                 20_000_000)
         traffic_ncu = {("PrimalOp", "tile"): 242.8e6, ("DualOp", "tile"): 187.9e6,
-                       ("PrimalOp", "vec"): 250.2e6, ("DualOp", "vec"): 194.8e6}
+                       ("PrimalOp", "vec"): 250.2e6, ("DualOp", "vec"): 189.6e6}
         tun = mx["tuning"]
 
         seg = tun.get("a_long_row_segments", 0)

@@ -26,7 +26,7 @@ def zipf(oracle):
     I = milp.int_idx
     xt = np.zeros(len(milp.c))
     xt[I] = np.round(rng.random(len(I)))
-    assert np.diff(milp.A.indptr).max() > 2 * 1024  # rows of three pieces and more
+    assert np.diff(milp.A.indptr).max() > 2048  # rows of two pieces (2,048 nonzeros a piece)
     return milp, xt, oracle.projector_inputs(milp)
 
 
